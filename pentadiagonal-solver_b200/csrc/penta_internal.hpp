@@ -1,0 +1,50 @@
+// penta_internal.hpp -- interfaces between the host dispatcher (C++) and the
+// kernel launchers (CUDA).  Nothing here crosses the library boundary.
+#pragma once
+#include <cuda_runtime_api.h>
+#include <cstddef>
+#include <type_traits>
+#include <vector>
+
+#include "penta_lines.h"
+
+namespace penta {
+
+template <typename F> struct SolveArgs {
+  const F *ds, *dl, *d, *du, *dw;
+  F *x;
+  Lines L;
+  void *scratch;         // caller's buffer (may be null when unused)
+  size_t scratch_bytes;  // its size
+  int *status;           // device word that kernels OR status bits into
+};
+
+// A compiled variant of the tiled Thomas kernel.
+struct TiledConfig {
+  int S;       // systems per CTA
+  int P;       // partitions (threads) per system: 1 or 2
+  bool contig; // contiguous (x) layout
+  int R;       // rows per ring slot
+  int stages;  // ring slots
+};
+
+// thomas_kernels.cu
+template <typename F>
+cudaError_t launch_thomas_global(const SolveArgs<F> &a, cudaStream_t stream);
+template <typename F>
+cudaError_t launch_thomas_tiled(const SolveArgs<F> &a, const TiledConfig &cfg,
+                                int max_ctas, cudaStream_t stream);
+template <typename F> size_t tiled_smem_bytes(const TiledConfig &cfg, long long n);
+template <typename F> int tiled_occupancy(const TiledConfig &cfg, long long n);
+template <typename F> const std::vector<TiledConfig> &tiled_configs();
+
+// penta_status.cu: address of the device status word of `device` (the
+// current device when the address is first taken).
+int *device_status_word(int device);
+
+// Bytes of caller scratch the global-scratch kernel needs.
+template <typename F> inline size_t thomas_global_scratch(const Lines &L) {
+  return (size_t)3 * (size_t)L.n * (size_t)L.n_sys * sizeof(F);
+}
+
+}  // namespace penta

@@ -1,0 +1,243 @@
+"""Python front end to libpentadsolver_b200.so through its C ABI (ctypes).
+
+Mirrors the reference's interface for the path (include/pentadsolver.hpp):
+``gpsv_batch`` takes the five diagonals and the in/out right-hand side as
+device arrays of one grid, the solve dimension, and a caller-owned scratch
+buffer of ``buffer_size`` bytes.  Arrays are torch CUDA tensors in C order
+whose last axis is the reference's ``t_dims[0]`` (the contiguous x axis);
+``dims`` are derived fastest-first exactly as the reference API takes them.
+
+There is no CPU fallback: every call goes to the CUDA library, and loading
+fails loudly when the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libpentadsolver_b200.so"
+
+SUCCESS = 0
+NOT_INITIALIZED = 1
+ALLOC_FAILED = 2
+INVALID_VALUE = 3
+EXECUTION_FAILED = 6
+INTERNAL_ERROR = 7
+ZERO_PIVOT = 9
+
+DIR_X, DIR_MIDDLE, DIR_OUTERMOST = 0, 1, 2
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_Z = ctypes.c_size_t
+_lib = None
+
+
+class PentadError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        super().__init__(f"{what}: {status_string(status)} ({status})")
+
+
+def lib() -> ctypes.CDLL:
+    """Load (once) and type the shared library."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is not built; run `make -C {HERE}`")
+    L = ctypes.CDLL(str(LIB_PATH))
+    L.pentadsolver_create.argtypes = [ctypes.POINTER(_P), _P, _I, _P]
+    L.pentadsolver_create.restype = None
+    L.pentadsolver_destroy.argtypes = [ctypes.POINTER(_P)]
+    L.pentadsolver_destroy.restype = None
+    for pre in ("D", "S"):
+        f = getattr(L, f"pentadsolver_{pre}_gpsv_batch_buffer_size_ext")
+        f.argtypes = [_P] * 7 + [_P, _I, _I]
+        f.restype = _Z
+        f = getattr(L, f"pentadsolver_{pre}_gpsv_batch")
+        f.argtypes = [_P] * 7 + [_P, _I, _I, _P]
+        f.restype = None
+        f = getattr(L, f"pentadsolver_{pre}_gpsv_batch_ex")
+        f.argtypes = [_P] * 7 + [_P, _I, _I, _P, _Z, _P]
+        f.restype = _I
+        f = getattr(L, f"pentadsolver_{pre}_gpsv_batch_two_buffer")
+        f.argtypes = [_P] * 7 + [_P, _I, _I, _P, _P]
+        f.restype = None
+        f = getattr(L, f"pentadsolver_{pre}_gpsv_batch_buffer_size_two_buffer")
+        f.argtypes = [_P] * 7 + [_P, _I, _I, ctypes.POINTER(_Z), ctypes.POINTER(_Z)]
+        f.restype = None
+    L.pentadsolver_kernel_that_ran.argtypes = [_I]
+    L.pentadsolver_kernel_that_ran.restype = ctypes.c_char_p
+    L.pentadsolver_kernel_that_ran_ex.argtypes = [_P, _I]
+    L.pentadsolver_kernel_that_ran_ex.restype = ctypes.c_char_p
+    L.pentadsolver_variant_that_ran.argtypes = [_P, _I]
+    L.pentadsolver_variant_that_ran.restype = ctypes.c_char_p
+    L.pentadsolver_buffer_size_ex.argtypes = [_P, _I, _P, _I, _I, ctypes.POINTER(_Z)]
+    L.pentadsolver_buffer_size_ex.restype = _I
+    L.pentadsolver_status_check.argtypes = [_P, _P, ctypes.POINTER(_I)]
+    L.pentadsolver_status_check.restype = _I
+    L.pentadsolver_set_algo.argtypes = [_P, _I, ctypes.c_char_p, _I]
+    L.pentadsolver_set_algo.restype = _I
+    L.pentadsolver_status_string.argtypes = [_I]
+    L.pentadsolver_status_string.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def status_string(status: int) -> str:
+    return lib().pentadsolver_status_string(int(status)).decode()
+
+
+def _dims(dims):
+    return (ctypes.c_int * len(dims))(*[int(v) for v in dims])
+
+
+def dims_of(t) -> list[int]:
+    """Reference-order dims (fastest first) of a C-order array."""
+    return [int(v) for v in reversed(tuple(t.shape))]
+
+
+def _elem_prefix(dtype) -> tuple[str, int]:
+    s = str(dtype)
+    if s.endswith("float64"):
+        return "D", 8
+    if s.endswith("float32"):
+        return "S", 4
+    raise TypeError(f"unsupported dtype {dtype}: float64 or float32")
+
+
+class Handle:
+    """A library context (``pentadsolver_create`` / ``pentadsolver_destroy``)."""
+
+    def __init__(self):
+        self._h = _P()
+        lib().pentadsolver_create(ctypes.byref(self._h), None, 0, None)
+
+    @property
+    def value(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().pentadsolver_destroy(ctypes.byref(self._h))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_algo(self, direction: int, algo: str | None, pcr_lanes: int = 0) -> None:
+        st = lib().pentadsolver_set_algo(self._h, int(direction),
+                                         None if algo is None else algo.encode(),
+                                         int(pcr_lanes))
+        if st != SUCCESS:
+            raise PentadError(st, "set_algo")
+
+    def kernel_that_ran(self, direction: int) -> str:
+        return lib().pentadsolver_kernel_that_ran_ex(self._h, int(direction)).decode()
+
+    def variant_that_ran(self, direction: int) -> str:
+        return lib().pentadsolver_variant_that_ran(self._h, int(direction)).decode()
+
+
+def _hval(handle):
+    if handle is None:
+        return None
+    return handle.value if isinstance(handle, Handle) else handle
+
+
+def buffer_size(dims, solvedim: int, elem_bytes: int = 8, handle=None) -> int:
+    out = ctypes.c_size_t(0)
+    st = lib().pentadsolver_buffer_size_ex(_hval(handle), int(elem_bytes), _dims(dims),
+                                           len(dims), int(solvedim), ctypes.byref(out))
+    if st != SUCCESS:
+        raise PentadError(st, "buffer_size")
+    return int(out.value)
+
+
+def kernel_that_ran(direction: int) -> str:
+    return lib().pentadsolver_kernel_that_ran(int(direction)).decode()
+
+
+def _ptr(t) -> int:
+    return int(t.data_ptr())
+
+
+def _check_arrays(arrs):
+    x = arrs[-1]
+    for a in arrs:
+        if not a.is_cuda or not a.is_contiguous():
+            raise ValueError("arrays must be contiguous CUDA tensors")
+        if a.dtype != x.dtype or tuple(a.shape) != tuple(x.shape):
+            raise ValueError("arrays must share dtype and shape")
+
+
+def gpsv_batch(ds, dl, d, du, dw, x, solvedim: int, buffer=None, stream=None,
+               handle=None, dims=None, check: bool = True) -> int:
+    """Solve in place along ``solvedim`` (``pentadsolver_{D,S}_gpsv_batch_ex``).
+
+    ``buffer`` is a CUDA tensor used as scratch (any dtype); ``stream`` a
+    ``torch.cuda.Stream`` or raw handle (default: torch's current stream).
+    Returns the status; raises on failure when ``check``.
+    """
+    import torch
+
+    _check_arrays((ds, dl, d, du, dw, x))
+    pre, _ = _elem_prefix(x.dtype)
+    dims = dims_of(x) if dims is None else list(dims)
+    if stream is None:
+        stream = torch.cuda.current_stream(x.device)
+    sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+    bptr, bbytes = (None, 0) if buffer is None else (_ptr(buffer),
+                                                     buffer.numel() * buffer.element_size())
+    fn = getattr(lib(), f"pentadsolver_{pre}_gpsv_batch_ex")
+    st = fn(_hval(handle), *(_ptr(a) for a in (ds, dl, d, du, dw, x)), _dims(dims),
+            len(dims), int(solvedim), bptr, bbytes, sp)
+    if check and st != SUCCESS:
+        raise PentadError(st, "gpsv_batch")
+    return st
+
+
+def gpsv_batch_legacy(ds, dl, d, du, dw, x, solvedim: int, buffer=None, handle=None,
+                      dims=None) -> None:
+    """The reference-named void entry point ``pentadsolver_{D,S}_gpsv_batch``
+    (legacy default stream, errors on stderr)."""
+    _check_arrays((ds, dl, d, du, dw, x))
+    pre, _ = _elem_prefix(x.dtype)
+    dims = dims_of(x) if dims is None else list(dims)
+    fn = getattr(lib(), f"pentadsolver_{pre}_gpsv_batch")
+    fn(_hval(handle), *(_ptr(a) for a in (ds, dl, d, du, dw, x)), _dims(dims), len(dims),
+       int(solvedim), None if buffer is None else _ptr(buffer))
+
+
+def status_check(stream=None, handle=None) -> tuple[int, int]:
+    """Synchronise and read/clear the device status bits: (status, bits)."""
+    sp = None
+    if stream is not None:
+        sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+    bits = ctypes.c_int(0)
+    st = lib().pentadsolver_status_check(_hval(handle), sp, ctypes.byref(bits))
+    return int(st), int(bits.value)
+
+
+def alloc_buffer(dims, solvedim: int, dtype, device="cuda"):
+    """A scratch tensor of ``buffer_size`` bytes (the caller owns scratch)."""
+    import torch
+
+    _, eb = _elem_prefix(dtype)
+    nbytes = max(buffer_size(dims, solvedim, eb), 256)
+    return torch.empty(nbytes, dtype=torch.uint8, device=device)
+
+
+def library_loaded_path() -> str:
+    return os.fspath(LIB_PATH)

@@ -1,0 +1,143 @@
+"""The C-ABI boundary, checked without a GPU.
+
+* libpentadsolver_b200.so loads and exports every entry point include/*.h
+  declares (C names through ctypes, the C++ overloads by their mangled names).
+* Sizing functions and argument validation are host logic: they answer
+  without touching a device.
+"""
+import re
+import shutil
+import subprocess
+from pathlib import Path
+
+import pytest
+
+import pentadsolver as ps
+
+REPO = Path(__file__).resolve().parent.parent
+INCLUDE = REPO / "include"
+
+
+def declared_c_functions():
+    names = set()
+    for h in INCLUDE.glob("*.h*"):
+        text = h.read_text()
+        # exported declarations carry PENTAD_API; inline wrappers do not
+        for m in re.finditer(r"PENTAD_API\s*(?:\n\s*)?[\w\s\*]*?\b(pentadsolver_\w+)\s*\(", text):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_headers_declare_the_reference_api():
+    names = declared_c_functions()
+    for ref_name in ("pentadsolver_create", "pentadsolver_destroy",
+                     "pentadsolver_D_gpsv_batch", "pentadsolver_S_gpsv_batch",
+                     "pentadsolver_D_gpsv_batch_buffer_size_ext",
+                     "pentadsolver_S_gpsv_batch_buffer_size_ext",
+                     "pentadsolver_kernel_that_ran"):
+        assert ref_name in names
+
+
+def test_library_exports_every_declared_c_symbol():
+    lib = ps.lib()
+    missing = [n for n in declared_c_functions()
+               if n != "pentadsolver_gpsv_batch" and n != "pentadsolver_gpsv_batch_buffer_size_ext"
+               and not hasattr(lib, n)]
+    assert not missing, missing
+
+
+@pytest.mark.skipif(shutil.which("nm") is None, reason="nm not available")
+def test_library_exports_cpp_overloads():
+    out = subprocess.run(["nm", "-D", "--defined-only", str(ps.LIB_PATH)],
+                         capture_output=True, text=True, check=True).stdout
+    # pentadsolver_gpsv_batch(void*, const double*x5, double*, const int*, int, int, void*)
+    for mangled in ("_Z23pentadsolver_gpsv_batchPvPKdS1_S1_S1_S1_PdPKiiiS_",
+                    "_Z23pentadsolver_gpsv_batchPvPKfS1_S1_S1_S1_PfPKiiiS_",
+                    "_Z39pentadsolver_gpsv_batch_buffer_size_extPvPKdS1_S1_S1_S1_S1_PKiii",
+                    "_Z39pentadsolver_gpsv_batch_buffer_size_extPvPKfS1_S1_S1_S1_S1_PKiii"):
+        assert mangled in out
+
+
+@pytest.mark.parametrize("dims,solvedim", [((256, 256, 256), 0), ((256, 256, 256), 1),
+                                           ((64, 32, 16), 2), ((200,), 0), ((8, 8), 1)])
+@pytest.mark.parametrize("elem", [8, 4])
+def test_buffer_size_covers_global_scratch(dims, solvedim, elem):
+    n_total = 1
+    for v in dims:
+        n_total *= v
+    b = ps.buffer_size(list(dims), solvedim, elem)
+    assert b >= 3 * n_total * elem
+    # the reference-named sizing functions agree
+    fn = getattr(ps.lib(), f"pentadsolver_{'D' if elem == 8 else 'S'}_gpsv_batch_buffer_size_ext")
+    assert fn(None, None, None, None, None, None, None, ps._dims(dims), len(dims), solvedim) == b
+    h, dv = ps.ctypes.c_size_t(7), ps.ctypes.c_size_t(0)
+    fn2 = getattr(ps.lib(), f"pentadsolver_{'D' if elem == 8 else 'S'}_gpsv_batch_buffer_size_two_buffer")
+    fn2(None, None, None, None, None, None, None, ps._dims(dims), len(dims), solvedim,
+        ps.ctypes.byref(h), ps.ctypes.byref(dv))
+    assert h.value == 0 and dv.value == b
+
+
+@pytest.mark.parametrize("dims,ndim,solvedim", [
+    ((16, 16, 16), 3, 3),      # solvedim out of range
+    ((16, 16, 16), 3, -1),
+    ((4, 16, 16), 3, 0),       # a line of 4 rows (the reference asserts > 4)
+    ((16, 0, 16), 3, 1),       # empty dimension
+    ((16,) * 9, 9, 0),         # rank above the maximum
+])
+def test_invalid_shapes_rejected_on_host(dims, ndim, solvedim):
+    out = ps.ctypes.c_size_t(0)
+    st = ps.lib().pentadsolver_buffer_size_ex(None, 8, ps._dims(dims), ndim, solvedim,
+                                              ps.ctypes.byref(out))
+    assert st == ps.INVALID_VALUE
+    # the solve entry point rejects the shape before any device work
+    st = ps.lib().pentadsolver_D_gpsv_batch_ex(None, 1, 1, 1, 1, 1, 1, ps._dims(dims), ndim,
+                                               solvedim, None, 0, None)
+    assert st == ps.INVALID_VALUE
+
+
+def test_null_arrays_rejected():
+    st = ps.lib().pentadsolver_D_gpsv_batch_ex(None, None, 1, 1, 1, 1, 1, ps._dims([8, 8]), 2,
+                                               0, None, 0, None)
+    assert st == ps.INVALID_VALUE
+
+
+def test_handles_and_selection_on_host():
+    with ps.Handle() as h:
+        assert h.value
+        assert h.kernel_that_ran(0) == "none"
+        h.set_algo(1, "naive")
+        h.set_algo(2, "thomas-pcr", pcr_lanes=2)
+        h.set_algo(0, None)
+        with pytest.raises(ps.PentadError):
+            h.set_algo(0, "bogus")
+        with pytest.raises(ps.PentadError):
+            h.set_algo(3, "naive")
+        with pytest.raises(ps.PentadError):
+            h.set_algo(0, "thomas-pcr", pcr_lanes=3)
+    assert ps.kernel_that_ran(5) == "none"
+
+
+def test_status_strings():
+    assert ps.status_string(ps.SUCCESS) == "success"
+    assert ps.status_string(ps.ZERO_PIVOT) == "zero pivot"
+    assert ps.status_string(ps.INVALID_VALUE) == "invalid value"
+
+
+def test_headers_compile_as_c_and_cpp(tmp_path):
+    cc = shutil.which("gcc")
+    cxx = shutil.which("g++")
+    if cc is None or cxx is None:
+        pytest.skip("no host compiler")
+    src = tmp_path / "t.c"
+    src.write_text('#include "pentadsolver.hpp"\n#include "pentadsolver_ext.h"\n'
+                   "int main(void){return 0;}\n")
+    subprocess.run([cc, "-std=c11", "-Wall", "-Werror", f"-I{INCLUDE}", "-c", str(src), "-o",
+                    str(tmp_path / "t.o")], check=True)
+    subprocess.run([cxx, "-std=c++17", "-Wall", "-Werror", f"-I{INCLUDE}", "-x", "c++", "-c",
+                    str(src), "-o", str(tmp_path / "t2.o")], check=True)
+    src2 = tmp_path / "t2.c"
+    src2.write_text('#include "pentadsolver_cuda.hpp"\nint main(void){return 0;}\n')
+    subprocess.run([cc, "-std=c11", "-Wall", "-Werror", f"-I{INCLUDE}", "-c", str(src2), "-o",
+                    str(tmp_path / "t3.o")], check=True)
+    subprocess.run([cxx, "-std=c++17", "-Wall", "-Werror", f"-I{INCLUDE}", "-x", "c++", "-c",
+                    str(src2), "-o", str(tmp_path / "t4.o")], check=True)

@@ -1,0 +1,257 @@
+"""GPU parity: the CUDA library through its C ABI against the oracle and the
+reference's golden data.
+
+Tolerances:
+  * golden fixtures: the reference's own per-element test tolerance
+    (test/catch_utils.hpp:19-22): rel 1e-13 or abs 1e-15 (FP64),
+    rel 1e-5 or abs 1e-6 (FP32);
+  * seeded grids: forward error max|x - x_ref| / max|x_ref| <= 1e-12 (FP64)
+    against the oracle and against the reference's compiled CPU solver,
+    <= 1e-5 (FP32) -- the definition of apps/fp32_accuracy_cuda.cu.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import fixtures
+import pentadsolver as ps
+from gpu_util import (NAMES, SELECTIONS, allclose_ref, direction, fwd_err, solve_dev,
+                      to_dev)
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+FWD_TOL = {np.float64: 1e-12, np.float32: 1e-5}
+
+
+def _selections_for(dirn):
+    return [s for s in SELECTIONS if s[0] != "transpose" or dirn == 0]
+
+
+@pytest.mark.parametrize("fam,solvedim", list(fixtures.all_fixture_cases()))
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_reference_fixtures_every_kernel(cuda, fam, solvedim, dtype):
+    fx = fixtures.load_fixture(fam, solvedim)
+    dims = fx["dims"]
+    dirn = direction(len(dims), solvedim)
+    expect = fx["u"] if dtype == np.float64 else fx["u_float"]
+    for label, algo, lanes in _selections_for(dirn):
+        co = {k: fx[k].astype(dtype) for k in NAMES}
+        dv = to_dev(co)
+        with ps.Handle() as h:
+            h.set_algo(dirn, algo, lanes)
+            solve_dev(dv, solvedim, dims=dims, handle=h)
+            ran = h.kernel_that_ran(dirn)
+        got = dv["x"].cpu().numpy()
+        ok, worst = allclose_ref(got, expect, dtype)
+        assert ok, f"{fam} solve{solvedim} {label} ({ran}): max diff {worst:.3e}"
+        want_family = {"auto": "thomas-pcr", "naive": "naive", "pcr-p1": "thomas-pcr",
+                       "pcr-p2": "thomas-pcr", "transpose": "transpose"}[label]
+        assert ran == want_family, (label, ran)
+
+
+@pytest.mark.parametrize("name", fixtures.REFRUNS)
+@pytest.mark.parametrize("tag,dtype", [("d", np.float64), ("s", np.float32)])
+def test_stored_reference_runs_x_then_y_then_z(cuda, name, tag, dtype):
+    z = fixtures.load_refrun(name)
+    dims = [int(v) for v in z["dims"]]
+    co = {k: z[f"{k}_{tag}"] for k in NAMES}
+    dv = to_dev(co)
+    for axis in range(3):
+        solve_dev(dv, axis, dims=dims)
+        got = dv["x"].cpu().numpy()
+        for which in ("orig", "simd"):
+            key = f"after{axis}_{which}_{tag}"
+            if key in z:
+                e = fwd_err(got, z[key])
+                assert e <= FWD_TOL[dtype], (name, axis, which, e)
+        # continue from the reference's state so errors do not compound
+        dv["x"].copy_(__import__("torch").from_numpy(z[f"after{axis}_orig_{tag}"]).to("cuda"))
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_config0_64cube_against_oracle_and_reference(cuda, dtype):
+    dims = (64, 64, 64)
+    co = fixtures.random_dominant(dims, 20240601, dtype)
+    dv = to_dev(co)
+    x_or = co["x"].copy()
+    x_ref = co["x"].copy()
+    for axis in range(3):
+        solve_dev(dv, axis)
+        oracle.solve(co["ds"], co["dl"], co["d"], co["du"], co["dw"], x_or, axis)
+        got = dv["x"].cpu().numpy()
+        assert fwd_err(got, x_or) <= FWD_TOL[dtype], axis
+        if oracle.ref_available("orig"):
+            oracle.ref_solve(co["ds"], co["dl"], co["d"], co["du"], co["dw"], x_ref, axis)
+            assert fwd_err(got, x_ref) <= FWD_TOL[dtype], axis
+
+
+ODD_DIMS = [(5,), (7,), (129,), (5, 5), (17, 6), (6, 17), (5, 7, 9), (33, 17, 6), (9, 5, 31),
+            (13, 11, 7, 5), (300, 3, 2)]
+
+
+@pytest.mark.parametrize("dims", ODD_DIMS)
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_odd_and_ragged_shapes_every_kernel(cuda, dims, dtype):
+    for solvedim in range(len(dims)):
+        if dims[solvedim] <= 4:
+            continue
+        dirn = direction(len(dims), solvedim)
+        co = fixtures.random_dominant(dims, 7 + solvedim, dtype)
+        ref = co["x"].copy()
+        oracle.solve(co["ds"], co["dl"], co["d"], co["du"], co["dw"], ref, solvedim)
+        for label, algo, lanes in _selections_for(dirn):
+            dv = to_dev(co)
+            with ps.Handle() as h:
+                h.set_algo(dirn, algo, lanes)
+                solve_dev(dv, solvedim, handle=h)
+            e = fwd_err(dv["x"].cpu().numpy(), ref)
+            assert e <= FWD_TOL[dtype], (dims, solvedim, label, e)
+
+
+@pytest.mark.parametrize("solvedim", [0, 1, 2])
+def test_nan_in_ignored_entries_changes_nothing(cuda, solvedim):
+    dims = (19, 12, 10)
+    co = fixtures.random_dominant(dims, 31, np.float64)
+    clean = {k: v.copy() for k, v in co.items()}
+    fixtures.zero_out_of_range(clean, solvedim)
+    dirty = {k: v.copy() for k, v in co.items()}
+    ax = 2 - solvedim
+
+    def sl(i):
+        s = [slice(None)] * 3
+        s[ax] = i
+        return tuple(s)
+
+    for name, rows in (("ds", [0, 1]), ("dl", [0]), ("du", [-1]), ("dw", [-2, -1])):
+        for r in rows:
+            dirty[name][sl(r)] = np.nan
+    dirn = direction(3, solvedim)
+    for label, algo, lanes in _selections_for(dirn):
+        outs = []
+        for c in (clean, dirty):
+            dv = to_dev(c)
+            with ps.Handle() as h:
+                h.set_algo(dirn, algo, lanes)
+                solve_dev(dv, solvedim, handle=h)
+            outs.append(dv["x"].cpu().numpy())
+        assert np.all(np.isfinite(outs[1])), label
+        assert np.array_equal(outs[0], outs[1]), label
+
+
+def test_zero_pivot_is_reported(cuda):
+    dims = (16, 8, 8)
+    co = fixtures.random_dominant(dims, 3, np.float64)
+    co["d"][2, 3, 0] = 0.0      # first row of one x line: pivot exactly zero
+    co["dl"][2, 3, 1] = 0.0
+    co["ds"][2, 3, 2] = 0.0
+    ps.status_check()           # clear
+    dv = to_dev(co)
+    solve_dev(dv, 0)
+    st, bits = ps.status_check()
+    assert st == ps.ZERO_PIVOT and bits & 1
+    st, bits = ps.status_check()
+    assert st == ps.SUCCESS and bits == 0
+
+
+def test_naive_rejects_short_buffer(cuda):
+    import torch
+
+    dims = (16, 16, 16)
+    co = fixtures.random_dominant(dims, 3, np.float64)
+    dv = to_dev(co)
+    small = torch.empty(1024, dtype=torch.uint8, device="cuda")
+    with ps.Handle() as h:
+        h.set_algo(1, "naive")
+        st = ps.gpsv_batch(*(dv[k] for k in NAMES), 1, buffer=small, handle=h, check=False)
+    assert st == ps.INVALID_VALUE
+
+
+def test_explicit_stream_and_legacy_entry_point(cuda):
+    import torch
+
+    dims = (48, 40, 36)
+    co = fixtures.random_dominant(dims, 11, np.float64)
+    ref = co["x"].copy()
+    for axis in range(3):
+        oracle.solve(co["ds"], co["dl"], co["d"], co["du"], co["dw"], ref, axis)
+    dv = to_dev(co)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        for axis in range(3):
+            solve_dev(dv, axis, stream=s)
+    s.synchronize()
+    assert fwd_err(dv["x"].cpu().numpy(), ref) <= 1e-12
+    # the reference-named void entry point on the legacy default stream
+    dv = to_dev(co)
+    buf = ps.alloc_buffer(list(dims), 0, torch.float64)
+    torch.cuda.synchronize()
+    for axis in range(3):
+        ps.gpsv_batch_legacy(*(dv[k] for k in NAMES), axis, buffer=buf)
+    torch.cuda.synchronize()
+    assert fwd_err(dv["x"].cpu().numpy(), ref) <= 1e-12
+
+
+def test_environment_selectors_and_kernel_record(cuda, monkeypatch):
+    import torch
+
+    dims = (24, 20, 18)
+    co = fixtures.random_dominant(dims, 12, np.float64)
+    ref = co["x"].copy()
+    for axis in range(3):
+        oracle.solve(co["ds"], co["dl"], co["d"], co["du"], co["dw"], ref, axis)
+    cases = [
+        ({"PENTA_XALGO": "naive"}, ("naive", "thomas-pcr", "thomas-pcr")),
+        ({"PENTA_XALGO": "transpose", "PENTA_YZALGO": "naive"}, ("transpose", "naive", "naive")),
+        ({"PENTA_YALGO": "thomas-pcr", "PENTA_YZALGO": "naive"}, ("thomas-pcr", "thomas-pcr", "naive")),
+        ({"PENTA_ZALGO": "legacy"}, ("thomas-pcr", "thomas-pcr", "naive")),
+        ({"PENTA_XALGO": "bogus"}, ("thomas-pcr", "thomas-pcr", "thomas-pcr")),
+        ({"PENTA_PCR_LANES": "1"}, ("thomas-pcr", "thomas-pcr", "thomas-pcr")),
+    ]
+    for env, expect in cases:
+        for k in ("PENTA_XALGO", "PENTA_YALGO", "PENTA_ZALGO", "PENTA_YZALGO", "PENTA_PCR_LANES"):
+            monkeypatch.delenv(k, raising=False)
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        dv = to_dev(co)
+        buf = ps.alloc_buffer(list(reversed(co["x"].shape)), 0, torch.float64)
+        for axis in range(3):
+            ps.gpsv_batch_legacy(*(dv[k] for k in NAMES), axis, buffer=buf)
+        torch.cuda.synchronize()
+        assert tuple(ps.kernel_that_ran(d) for d in range(3)) == expect, env
+        assert fwd_err(dv["x"].cpu().numpy(), ref) <= 1e-12, env
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("solvedim", [0, 1, 2])
+def test_256cube_properties(cuda, solvedim):
+    """Full-size checks at 256^3 FP64: agreement with the oracle, with the
+    global-scratch kernel, and linearity in the right-hand side."""
+    import torch
+
+    dims = (256, 256, 256)
+    co = fixtures.random_dominant(dims, 77, np.float64)
+    ref = co["x"].copy()
+    oracle.solve(co["ds"], co["dl"], co["d"], co["du"], co["dw"], ref, solvedim)
+    dv = to_dev(co)
+    b = dv["x"].clone()
+    solve_dev(dv, solvedim)
+    x_auto = dv["x"].clone()
+    assert fwd_err(x_auto.cpu().numpy(), ref) <= 1e-12
+    # naive kernel agrees
+    dirn = direction(3, solvedim)
+    with ps.Handle() as h:
+        h.set_algo(dirn, "naive")
+        dv["x"].copy_(b)
+        solve_dev(dv, solvedim, handle=h)
+    assert fwd_err(dv["x"].cpu().numpy(), x_auto.cpu().numpy()) <= 1e-12
+    # linearity: A^-1 (2 b + b') = 2 A^-1 b + A^-1 b'
+    b2 = torch.from_numpy(np.random.default_rng(5).uniform(-1, 1, b.shape)).cuda()
+    dv["x"].copy_(b2)
+    solve_dev(dv, solvedim)
+    x2 = dv["x"].clone()
+    dv["x"].copy_(2 * b + b2)
+    solve_dev(dv, solvedim)
+    lin = (2 * x_auto + x2).cpu().numpy()
+    assert fwd_err(dv["x"].cpu().numpy(), lin) <= 1e-12
