@@ -1,0 +1,425 @@
+#!/usr/bin/env python3
+"""Benchmark: the constant-coefficient ADI sweep on a 256^3 FP64 grid.
+
+Workload (one "step"): one ADI run of 50 iterations, each iteration solving
+the pentadiagonal systems along x, then y, then z of a 256^3 FP64 grid in
+place, with the general kernels reading full coefficient arrays
+(ds = dw = -r/12, dl = du = 16r/12, d = 1 + 30r/12, r = 0.5; initial field
+U(-1,1) from a fixed seed).  Every solve goes through the library's C ABI
+(libpentadsolver_b200.so), automatic kernel selection.
+
+Metric: algorithmic HBM bandwidth, 7 arrays x 8 B = 56 B per grid point per
+axis (5 coefficient arrays + RHS read, solution written), over the device
+time of the step.  Inputs are 7 x 128 MiB per axis, larger than the 126 MB
+L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun every rank solves its own grid (independent replicas: the
+path has no data exchange), timed with CUDA events between barriers; the
+reported time is the max over ranks and `value` counts all ranks' bytes.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+PKG = REPO / "pentadiagonal-solver_b200"
+for p in (str(PKG), str(REPO)):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+N_DEFAULT = 256
+ITERS = 50
+R_DIFF = 0.5
+SEED = 2024
+BYTES_PER_POINT_AXIS = 7 * 8
+METRIC = "ADI sweep HBM GB/s (256^3 FP64, 50 x/y/z iterations per step)"
+
+
+def peak_hbm():
+    f = REPO / "MEASURED_PEAKS.json"
+    try:
+        v = float(json.loads(f.read_text())["hbm_gbs"])
+        return v, "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_record():
+    """Per-launch DRAM bytes of the solve kernels from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    f = REPO / "profiles" / "traffic.json"
+    try:
+        return json.loads(f.read_text())
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons while timing."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        rows = []
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append({"sm": float(parts[1]), "max": float(parts[2]),
+                             "power": float(parts[3]) if parts[3] not in ("[N/A]", "") else 0.0,
+                             "hw": parts[5], "hwt": parts[6], "swt": parts[7], "pcap": parts[8]})
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        loaded = [r for r in rows if r["power"] > 200.0] or rows
+        reasons = set()
+        for r in loaded:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"),
+                              ("swt", "sw_thermal_slowdown"), ("pcap", "sw_power_cap")):
+                if r[key].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in loaded),
+                "sm_max_mhz": max(r["max"] for r in rows), "reasons": sorted(reasons),
+                "samples": len(loaded)}
+
+
+def adi_problem(n: int, device, dtype):
+    import torch
+
+    g = torch.Generator(device="cpu").manual_seed(SEED)
+    shape = (n, n, n)
+    field = (torch.rand(shape, generator=g, dtype=torch.float64) * 2.0 - 1.0).to(dtype)
+    c = {
+        "ds": -R_DIFF / 12.0, "dl": 16.0 * R_DIFF / 12.0, "d": 1.0 + 30.0 * R_DIFF / 12.0,
+        "du": 16.0 * R_DIFF / 12.0, "dw": -R_DIFF / 12.0,
+    }
+    host = {k: torch.full(shape, v, dtype=dtype) for k, v in c.items()}
+    host["x"] = field
+    dev = {k: v.to(device) for k, v in host.items()}
+    return host, dev
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import pentadsolver as ps
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n
+    dims = [n, n, n]
+    host, d = adi_problem(n, dev, torch.float64)
+    names = ("ds", "dl", "d", "du", "dw")
+    buf = ps.alloc_buffer(dims, 0, torch.float64, dev)
+    stream = torch.cuda.Stream(device=dev)
+    handle = ps.Handle()
+
+    def solve(axis, x):
+        ps.gpsv_batch(*(d[k] for k in names), x, axis, buffer=buf, stream=stream,
+                      handle=handle)
+
+    def step(x, dir_events=None):
+        for it in range(ITERS):
+            for axis in range(3):
+                if dir_events is not None and it == 0:
+                    dir_events[axis][0].record(stream)
+                solve(axis, x)
+                if dir_events is not None and it == 0:
+                    dir_events[axis][1].record(stream)
+
+    x = d["x"]
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step(x)
+    stream.synchronize()
+    ran = [handle.kernel_that_ran(a) for a in range(3)]
+    variants = [handle.variant_that_ran(a) for a in range(3)]
+
+    # ---- timed region: K steps, device time ---------------------------------
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    dir_ev = [[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(3)]
+              for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for k in range(args.steps):
+            step(x, dir_ev[k])
+        ev1.record(stream)
+        stream.synchronize()
+    torch.cuda.synchronize()
+    ms_total = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+        dist.barrier()
+    ms_step = ms_total / args.steps
+    per_dir_ms = [statistics.mean(dir_ev[k][a][0].elapsed_time(dir_ev[k][a][1])
+                                  for k in range(args.steps)) for a in range(3)]
+    alg_bytes_step = BYTES_PER_POINT_AXIS * n ** 3 * 3 * ITERS
+    value = world * alg_bytes_step / (ms_step * 1e-3) / 1e9
+
+    # ---- end to end through the public API with host buffers ----------------
+    pinned = {k: v.pin_memory() for k, v in host.items()}
+    out = torch.empty_like(pinned["x"]).pin_memory()
+    h2d = sum(v.numel() * v.element_size() for v in pinned.values())
+    d2h = out.numel() * out.element_size()
+    e2e_steps = max(2, min(args.steps, 5))
+
+    def e2e_step():
+        for k in ("ds", "dl", "d", "du", "dw", "x"):
+            d[k].copy_(pinned[k], non_blocking=True)
+        step(d["x"])
+        out.copy_(d["x"], non_blocking=True)
+
+    with torch.cuda.stream(stream):
+        e2e_step()
+    stream.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            e2e_step()
+        e1.record(stream)
+    stream.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * alg_bytes_step / (e2e_ms * 1e-3) / 1e9
+
+    # ---- roofline of the dominant kernel -------------------------------------
+    dom = max(range(3), key=lambda a: per_dir_ms[a])
+    achieved = BYTES_PER_POINT_AXIS * n ** 3 / (per_dir_ms[dom] * 1e-3) / 1e9
+    peak, peak_src = peak_hbm()
+    tr = traffic_record()
+    traffic = None
+    if tr is not None:
+        rec = tr.get(f"dir{dom}")
+        if rec is not None and rec.get("n") == n and rec.get("variant") == variants[dom]:
+            traffic = rec.get("bytes_per_launch")
+
+    result = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (config 1 coefficients, seeded U(-1,1) field)",
+        "config": {
+            "workload": "adi_256cube_fp64_general_50iter",
+            "grid": dims,
+            "iters_per_step": ITERS,
+            "kernel_family": ran,
+            "kernel_variant": variants,
+            "per_direction_ms": [round(v, 4) for v in per_dir_ms],
+            "l2": "no flush: 7 x 128 MiB per axis exceeds the 126 MB L2",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        },
+        "clocks": clk.summary(),
+        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 3)},
+        "gpu_launches": args.steps * ITERS * 3,
+        "roofline": {
+            "bound": "hbm",
+            "kernel": f"dir{dom} {variants[dom]}",
+            "achieved": round(achieved, 1),
+            "peak": peak,
+            "peak_source": peak_src,
+            "unit": "GB/s",
+            "frac": round(achieved / peak, 4),
+            "traffic": traffic,
+            "algorithmic_bytes_per_launch": BYTES_PER_POINT_AXIS * n ** 3,
+        },
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(n, budget_s=args.cpu_seconds)
+    handle.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result))
+
+
+def _cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_problem(n):
+    import numpy as np
+
+    rng = np.random.default_rng(SEED)
+    shape = (n, n, n)
+    co = {
+        "ds": np.full(shape, -R_DIFF / 12.0), "dl": np.full(shape, 16.0 * R_DIFF / 12.0),
+        "d": np.full(shape, 1.0 + 30.0 * R_DIFF / 12.0), "du": np.full(shape, 16.0 * R_DIFF / 12.0),
+        "dw": np.full(shape, -R_DIFF / 12.0), "x": rng.uniform(-1.0, 1.0, shape),
+    }
+    return co
+
+
+def cpu_solver():
+    """The reference's own CPU solver (compiled from its tree into oracle/_ref)
+    or, when that build is absent, the oracle port."""
+    from oracle import oracle
+
+    if oracle.ref_available("simd"):
+        return (lambda co, axis: oracle.ref_solve(co["ds"], co["dl"], co["d"], co["du"],
+                                                  co["dw"], co["x"], axis, which="simd"),
+                "reference", "src/cpu/singlenode/pentad_cpu.cpp (OpenMP+AVX2)")
+    return (lambda co, axis: oracle.solve(co["ds"], co["dl"], co["d"], co["du"], co["dw"],
+                                          co["x"], axis),
+            "port", "oracle/penta_oracle.c")
+
+
+def cpu_baseline(n, budget_s=12.0, max_iters=50):
+    from oracle import oracle
+
+    threads = _cpu_threads()
+    oracle.set_threads(threads)
+    co = cpu_problem(n)
+    fn, kind, what = cpu_solver()
+    for axis in range(3):  # warm-up (page faults, thread pool)
+        fn(co, axis)
+    t0 = time.perf_counter()
+    iters = 0
+    while iters < max_iters and (time.perf_counter() - t0) < budget_s:
+        for axis in range(3):
+            fn(co, axis)
+        iters += 1
+    dt = time.perf_counter() - t0
+    gbs = BYTES_PER_POINT_AXIS * n ** 3 * 3 * iters / dt / 1e9
+    return {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind,
+            "sample": f"{iters} ADI iterations (x,y,z) of the {n}^3 FP64 grid, {what}, "
+                      f"{dt:.1f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle
+
+    threads = _cpu_threads()
+    oracle.set_threads(threads)
+    n = args.n
+    co = cpu_problem(n)
+    fn, kind, what = cpu_solver()
+    for _ in range(args.warmup):
+        for axis in range(3):
+            fn(co, axis)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for axis in range(3):
+            fn(co, axis)
+    dt = time.perf_counter() - t0
+    ms_step = dt * 1e3 / args.steps
+    value = BYTES_PER_POINT_AXIS * n ** 3 * 3 / (ms_step * 1e-3) / 1e9
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    print(json.dumps({
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (config 1 coefficients, seeded U(-1,1) field)",
+        "config": {"workload": "adi_256cube_fp64_general_50iter", "grid": [n, n, n],
+                   "step": "one ADI iteration (x,y,z) of the workload, host cores",
+                   "parallelism": "host cores"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads,
+                         "kind": kind, "sample": f"{args.steps} ADI iterations, {what}"},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

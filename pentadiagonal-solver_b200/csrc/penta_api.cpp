@@ -16,6 +16,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <unordered_set>
 
 #include "pentad_common.hpp"
@@ -69,6 +70,7 @@ struct Context {
   int forced_lanes[3] = {0, 0, 0};
   std::atomic<const char *> ran[3] = {{kNone}, {kNone}, {kNone}};
   std::string variant[3];
+  std::unordered_map<long long, int> occ_cache;  // (variant, n) -> CTAs/SM
 
   bool init() {  // idempotent; needs a usable device
     if (device >= 0) return true;
@@ -196,44 +198,50 @@ int selected_lanes(Context &ctx, int dir) {
   return ctx.forced_lanes[dir];
 }
 
-// Preferred tiled variants, best first, per precision and layout.
+// The on-chip (tiled) variant for a shape: among the compiled variants of
+// this precision, layout and partition count whose shared memory fits, the
+// one with the most resident CTAs per SM (capped at 4), then the deepest
+// ring.  Occupancy queries are cached per (variant, n).
 template <typename F>
 bool pick_tiled(Context &ctx, const Lines &L, bool contig, int P,
-                TiledConfig &out) {
-  static const TiledConfig pref_d_strided[] = {
-      {16, 2, false, 1, 8}, {8, 2, false, 1, 8}, {32, 1, false, 1, 6}};
-  static const TiledConfig pref_d_contig[] = {
-      {16, 2, true, 2, 4}, {16, 2, true, 4, 2}, {8, 2, true, 8, 2},
-      {16, 1, true, 4, 2}};
-  static const TiledConfig pref_s_strided[] = {
-      {32, 2, false, 1, 8}, {16, 2, false, 1, 8}, {32, 1, false, 1, 8}};
-  static const TiledConfig pref_s_contig[] = {
-      {16, 2, true, 4, 4}, {16, 2, true, 8, 2}, {32, 2, true, 4, 2},
-      {32, 1, true, 4, 2}};
-  const bool dbl = sizeof(F) == 8;
-  const TiledConfig *list;
-  size_t cnt;
-  if (dbl) {
-    list = contig ? pref_d_contig : pref_d_strided;
-    cnt = contig ? std::size(pref_d_contig) : std::size(pref_d_strided);
-  } else {
-    list = contig ? pref_s_contig : pref_s_strided;
-    cnt = contig ? std::size(pref_s_contig) : std::size(pref_s_strided);
+                TiledConfig &out, int &occ_out) {
+  if (L.n * L.n_sys >= (1LL << 31)) return false;  // 32-bit in-tile offsets
+  const std::vector<TiledConfig> &all = tiled2_configs<F>();
+  int best = -1, best_score = -1, best_occ = 0;
+  for (size_t i = 0; i < all.size(); ++i) {
+    const TiledConfig &c = all[i];
+    if (c.contig != contig || (P != 0 && c.P != P)) continue;
+    if (tiled2_smem_bytes<F>(c, L.n) > (size_t)ctx.smem_optin) continue;
+    int occ;
+    const long long key = ((long long)i << 40) | (L.n << 1) | (sizeof(F) == 8);
+    {
+      std::lock_guard<std::mutex> lock(ctx.mu);
+      auto it = ctx.occ_cache.find(key);
+      occ = (it != ctx.occ_cache.end()) ? it->second : -1;
+    }
+    if (occ < 0) {
+      occ = tiled2_occupancy<F>(c, L.n);
+      std::lock_guard<std::mutex> lock(ctx.mu);
+      ctx.occ_cache[key] = occ;
+    }
+    if (occ <= 0) continue;
+    const int score = std::min(occ, 4) * 1000 + c.stages * c.R;
+    if (score > best_score) {
+      best_score = score;
+      best = (int)i;
+      best_occ = occ;
+    }
   }
-  for (size_t i = 0; i < cnt; ++i) {
-    const TiledConfig &c = list[i];
-    if (P != 0 && c.P != P) continue;
-    if (tiled_smem_bytes<F>(c, L.n) > (size_t)ctx.smem_optin) continue;
-    out = c;
-    return true;
-  }
-  return false;
+  if (best < 0) return false;
+  out = all[best];
+  occ_out = best_occ;
+  return true;
 }
 
 std::string tiled_variant_name(const TiledConfig &c) {
   char buf[96];
-  std::snprintf(buf, sizeof buf, "thomas-pcr:tiled S%d P%d R%d x%d%s", c.S,
-                c.P, c.R, c.stages, c.contig ? " contig" : "");
+  std::snprintf(buf, sizeof buf, "thomas-pcr:tiled P%d S%d R%d x%d%s", c.P,
+                c.S, c.R, c.stages, c.contig ? " contig" : "");
   return buf;
 }
 
@@ -289,8 +297,9 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
   };
   auto run_tiled = [&](int P, const char *family) -> int {
     TiledConfig cfg{};
-    if (!pick_tiled<F>(ctx, sh.L, contig, P, cfg)) return 0;  // declined
-    err = launch_thomas_tiled<F>(a, cfg, 0, stream);
+    int occ = 0;
+    if (!pick_tiled<F>(ctx, sh.L, contig, P, cfg, occ)) return 0;  // declined
+    err = launch_tiled2<F>(a, cfg, occ * ctx.sm_count, stream);
     if (err != cudaSuccess) {
       if (debug)
         std::fprintf(stderr, "[penta] %s launch declined: %s -- falling back\n",

@@ -27,6 +27,52 @@ template <typename F> __device__ __forceinline__ bool bad_pivot(F dd) {
   return !(dd != F(0)) || !isfinite(dd);
 }
 
+template <typename F> struct Carry {
+  F u1, u2, w1, w2, y1, y2;
+  __device__ __forceinline__ void zero() {
+    u1 = u2 = w1 = w2 = y1 = y2 = F(0);
+  }
+};
+
+// Reciprocal by Newton-Raphson refinement of the hardware approximation:
+// r <- r + r (1 - d r) doubles the number of correct bits per step, so two
+// steps take the ~20-bit rcp.approx.ftz.f64 seed past double precision (the
+// result is within an ulp or two of 1/d, not necessarily correctly rounded).
+// One step suffices from the single-precision seed.  A zero, infinite or NaN
+// pivot gives a non-finite result, which the kernels report.
+__device__ __forceinline__ double rcp_nr(double d) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+  double e = fma(-d, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-d, r, 1.0);
+  return fma(r, e, r);
+}
+__device__ __forceinline__ float rcp_nr(float d) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+  const float e = fmaf(-d, r, 1.0f);
+  return fmaf(r, e, r);
+}
+
+// Forward elimination of one row whose couplings are already masked; carries
+// as for fwd_row below.  `bad` collects non-finite reciprocals (zero pivots).
+template <typename F>
+__device__ __forceinline__ void fwd_row_fast(F ds, F dl, F d, F du, F dw, F b,
+                                             Carry<F> &c, F &du2, F &dw2,
+                                             F &x2, bool &bad) {
+  const F ddl = dl - ds * c.u2;
+  const F dd = d - ds * c.w2 - ddl * c.u1;
+  const F inv = rcp_nr(dd);
+  bad |= !isfinite(inv);
+  du2 = (du - ddl * c.w1) * inv;
+  dw2 = dw * inv;
+  x2 = (b - ds * c.y2 - ddl * c.y1) * inv;
+  c.u2 = c.u1; c.u1 = du2;
+  c.w2 = c.w1; c.w1 = dw2;
+  c.y2 = c.y1; c.y1 = x2;
+}
+
 // Zero the out-of-range couplings of row i of an n-row system.
 template <typename F>
 __device__ __forceinline__ void mask_row(long long i, long long n, F &ds,
@@ -44,13 +90,6 @@ __device__ __forceinline__ void mask_row(long long i, long long n, F &ds,
 //   in : ds dl d du dw b  of row i,  carries (u1,u2) = du2[i-1], du2[i-2],
 //        (w1,w2) = dw2[i-1], dw2[i-2], (y1,y2) = x2[i-1], x2[i-2]
 //   out: du2[i], dw2[i], x2[i] (also shifted into the carries)
-template <typename F> struct Carry {
-  F u1, u2, w1, w2, y1, y2;
-  __device__ __forceinline__ void zero() {
-    u1 = u2 = w1 = w2 = y1 = y2 = F(0);
-  }
-};
-
 template <typename F>
 __device__ __forceinline__ void fwd_row(F ds, F dl, F d, F du, F dw, F b,
                                         Carry<F> &c, F &du2, F &dw2, F &x2,
@@ -101,13 +140,14 @@ template <int BYTES>
 __device__ __forceinline__ void cp_async_ca(void *dst_smem, const void *src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(
                    smem_u32(dst_smem)),
-               "l"(src), "n"(BYTES));
+               "l"(src), "n"(BYTES)
+               : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;\n" ::);
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 template <int N> __device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 }  // namespace penta

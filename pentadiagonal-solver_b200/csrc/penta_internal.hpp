@@ -31,12 +31,14 @@ struct TiledConfig {
 // thomas_kernels.cu
 template <typename F>
 cudaError_t launch_thomas_global(const SolveArgs<F> &a, cudaStream_t stream);
+
+// tiled_kernels.cu (on-chip Thomas, one warp per CTA; S = 32 / P)
+template <typename F> const std::vector<TiledConfig> &tiled2_configs();
+template <typename F> size_t tiled2_smem_bytes(const TiledConfig &cfg, long long n);
+template <typename F> int tiled2_occupancy(const TiledConfig &cfg, long long n);
 template <typename F>
-cudaError_t launch_thomas_tiled(const SolveArgs<F> &a, const TiledConfig &cfg,
-                                int max_ctas, cudaStream_t stream);
-template <typename F> size_t tiled_smem_bytes(const TiledConfig &cfg, long long n);
-template <typename F> int tiled_occupancy(const TiledConfig &cfg, long long n);
-template <typename F> const std::vector<TiledConfig> &tiled_configs();
+cudaError_t launch_tiled2(const SolveArgs<F> &a, const TiledConfig &cfg,
+                          int grid, cudaStream_t stream);
 
 // penta_status.cu: address of the device status word of `device` (the
 // current device when the address is first taken).
