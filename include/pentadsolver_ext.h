@@ -61,4 +61,29 @@ EXTERN_C PENTAD_API const char *pentadsolver_variant_that_ran(pentadsolver_handl
 
 EXTERN_C PENTAD_API const char *pentadsolver_status_string(pentadStatus_t status);
 
+/* No counterpart in the reference.  An FP64 solve that allocates nothing and
+ * takes no scratch buffer, for callers that cannot call cudaMalloc around a
+ * solve: applications whose device memory is all owned by their own pool,
+ * solve loops where cudaMalloc/cudaFree would synchronise the device, and code
+ * written against the reference's CPU interface that passes no t_buffer.  It
+ * runs the global-scratch Thomas kernel with its scratch in a fixed device
+ * array of PENTADSOLVER_NOALLOC_MAX_BYTES that the library carries on every
+ * GPU that loads it, until the process exits.  Limits and rules:
+ *   - the grid may have at most PENTADSOLVER_NOALLOC_MAX_BYTES / 24 points
+ *     (699,050; e.g. 88^3); larger grids return PENTAD_STATUS_INVALID_VALUE
+ *     and a message on stderr, before any device work;
+ *   - all calls on a device share the array: calls that may overlap on the
+ *     GPU (unordered streams, several host threads) race and corrupt each
+ *     other's results; nothing needs clearing between ordered calls;
+ *   - the first call on each device takes the array's device address
+ *     (cudaGetSymbolAddress) with that device current, so make that first
+ *     call before any stream capture on the device.
+ * Asynchronous on `stream` (a cudaStream_t, or NULL for the legacy default
+ * stream); arguments otherwise as pentadsolver_D_gpsv_batch. */
+#define PENTADSOLVER_NOALLOC_MAX_BYTES (16u * 1024u * 1024u)
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_D_gpsv_batch_noalloc(
+    pentadsolver_handle_t handle, const double *ds, const double *dl,
+    const double *d, const double *du, const double *dw, double *x,
+    const int *t_dims, int t_ndim, int t_solvedim, void *stream);
+
 #endif /* PENTADSOLVER_EXT_H_INCLUDED */
