@@ -238,6 +238,43 @@ bool pick_tiled(Context &ctx, const Lines &L, bool contig, int P,
   return true;
 }
 
+// The TMA-fed strided variant: most resident CTAs (capped at 4), then the
+// deepest ring.
+template <typename F>
+bool pick_tma(Context &ctx, const SolveArgs<F> &a, TmaConfig &out, int &occ_out) {
+  if (!tma_supported<F>(a)) return false;
+  const std::vector<TmaConfig> &all = tma_configs<F>();
+  int best = -1, best_score = -1, best_occ = 0;
+  for (size_t i = 0; i < all.size(); ++i) {
+    const TmaConfig &c = all[i];
+    if (tma_smem_bytes<F>(c, a.L.n) > (size_t)ctx.smem_optin) continue;
+    int occ;
+    const long long key =
+        (1LL << 62) | ((long long)i << 40) | (a.L.n << 1) | (sizeof(F) == 8);
+    {
+      std::lock_guard<std::mutex> lock(ctx.mu);
+      auto it = ctx.occ_cache.find(key);
+      occ = (it != ctx.occ_cache.end()) ? it->second : -1;
+    }
+    if (occ < 0) {
+      occ = tma_occupancy<F>(c, a.L.n);
+      std::lock_guard<std::mutex> lock(ctx.mu);
+      ctx.occ_cache[key] = occ;
+    }
+    if (occ <= 0) continue;
+    const int score = std::min(occ, 4) * 1000 + c.stages * c.R;
+    if (score > best_score) {
+      best_score = score;
+      best = (int)i;
+      best_occ = occ;
+    }
+  }
+  if (best < 0) return false;
+  out = all[best];
+  occ_out = best_occ;
+  return true;
+}
+
 std::string tiled_variant_name(const TiledConfig &c) {
   char buf[96];
   std::snprintf(buf, sizeof buf, "thomas-pcr:tiled P%d S%d R%d x%d%s", c.P,
@@ -324,6 +361,24 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
     case Algo::Auto:
     default: {
       const int P = (lanes == 1) ? 1 : 2;
+      if (!contig && P == 2 && !env_flag("PENTA_NO_TMA")) {
+        TmaConfig tc{};
+        int occ = 0;
+        if (pick_tma<F>(ctx, a, tc, occ)) {
+          err = launch_tma<F>(a, tc, occ * ctx.sm_count, stream);
+          if (err == cudaSuccess) {
+            char buf[96];
+            std::snprintf(buf, sizeof buf, "thomas-pcr:tma P2 S16 R%d x%d/%d",
+                          tc.R, tc.stages, tc.xstages);
+            record(ctx, dir, "thomas-pcr", buf);
+            return PENTAD_STATUS_SUCCESS;
+          }
+          if (debug)
+            std::fprintf(stderr, "[penta] tma launch declined: %s -- falling back\n",
+                         cudaGetErrorString(err));
+          cudaGetLastError();
+        }
+      }
       if (run_tiled(P, "thomas-pcr")) return PENTAD_STATUS_SUCCESS;
       if (P == 1 && run_tiled(2, "thomas-pcr")) return PENTAD_STATUS_SUCCESS;
       break;

@@ -40,6 +40,20 @@ template <typename F>
 cudaError_t launch_tiled2(const SolveArgs<F> &a, const TiledConfig &cfg,
                           int grid, cudaStream_t stream);
 
+// A compiled variant of the TMA-fed strided kernel (tma_kernels.cu).
+struct TmaConfig {
+  int R;        // rows per ring stage
+  int stages;   // ring stages
+  int xstages;  // stages of the x2 read-back ring
+};
+template <typename F> const std::vector<TmaConfig> &tma_configs();
+template <typename F> size_t tma_smem_bytes(const TmaConfig &c, long long n);
+template <typename F> int tma_occupancy(const TmaConfig &c, long long n);
+template <typename F> bool tma_supported(const SolveArgs<F> &a);
+template <typename F>
+cudaError_t launch_tma(const SolveArgs<F> &a, const TmaConfig &c, int grid,
+                       cudaStream_t stream);
+
 // penta_status.cu: address of the device status word of `device` (the
 // current device when the address is first taken).
 int *device_status_word(int device);

@@ -23,6 +23,7 @@ namespace penta {
 // Status bits kernels OR into the per-device status word.
 enum : int {
   STATUS_ZERO_PIVOT_BIT = 1,  // a pivot was exactly zero or not finite
+  STATUS_TIMEOUT_BIT = 2,     // a bounded wait inside a kernel ran out
 };
 
 struct Lines {

@@ -1,0 +1,514 @@
+// tma_kernels.cu -- the on-chip Thomas kernel for the strided (y, z)
+// directions, fed by TMA.
+//
+// Same algorithm as tiled_kernels.cu with P = 2 (each of S = 16 systems per
+// warp split at row m = ceil(n/2), upper half eliminated downwards, lower half
+// upwards on the mirrored band, 4x4 interface solve by warp shuffles), with
+// three changes that cut the instructions a warp spends per row and the shared
+// memory it needs per system:
+//
+//  * Loads: one lane issues, per ring stage, 12 tensor-tile copies
+//    (cp.async.bulk.tensor.3d: 6 arrays x 2 halves, 16 systems x R rows each)
+//    that complete on one mbarrier.  The lower half's tiles are taken from the
+//    mirrored arrays (dw, du, d, dl, ds, rhs), so every lane runs the same
+//    downward recurrence without selects.  Each wait on an mbarrier is bounded;
+//    a wait that runs out raises STATUS_TIMEOUT_BIT and the kernel returns.
+//  * The forward-substituted right-hand side x2 is written in place into x
+//    (the right-hand side of that row has just been consumed) and read back,
+//    most recently written first, in the backward sweep through a small
+//    cp.async ring.  It makes an L2 round trip instead of occupying shared
+//    memory; the final solution overwrites the same lines, so HBM still sees
+//    one write per point.  Shared memory per system is 16 B/row (du2, dw2).
+//  * Stages of R rows are unrolled, with the first-row couplings zeroed in
+//    shared memory once per tile rather than masked per row.
+//
+// Tensor view: the array as a 3-D tensor {inner, n, outer} (element strides
+// 1, inner, inner*n), tile {16, R, 1} at (system offset in the run, first row,
+// run).  TMA requires a 16-byte aligned base, inner * sizeof(F) a multiple of
+// 16 and a 16-byte aligned innermost coordinate (the system offset is a
+// multiple of 16); the host checks all three and otherwise uses the cp.async
+// kernel.  Rows outside [0, n) read as zeros (never consumed).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "penta_device.cuh"
+#include "penta_internal.hpp"
+
+namespace penta {
+namespace {
+
+constexpr int TS = 16;                 // systems per warp
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile(
+      "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
+          smem_u32(bar)),
+      "r"(bytes)
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait: false when the barrier did not complete within ~2 s.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (global_ns() - t0 > 2000000000ull) return false;
+  return true;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map,
+                                            uint64_t *bar, int c0, int c1,
+                                            int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2),
+      "r"(smem_u32(bar))
+      : "memory");
+}
+
+template <typename F, int R, int STAGES, int XST>
+struct TmaGeom {
+  static constexpr int SE = 6 * 2 * R * TS;   // ring stage (elements)
+  static constexpr int XE = R * 32;           // x2 ring stage (elements)
+  static size_t smem_bytes(long long n) {
+    // [ring][du2,dw2 interleaved: n x 2 x 16][x2 ring][full, empty barriers]
+    return (size_t)((long long)STAGES * SE + n * 2 * TS + (long long)XST * XE) *
+               sizeof(F) +
+           2 * STAGES * sizeof(uint64_t);
+  }
+};
+
+struct TmaMaps {
+  CUtensorMap m[6];  // ds, dl, d, du, dw, x
+};
+
+// One row of forward elimination (couplings already masked); as fwd_row_fast
+// without the per-row pivot check -- a zero pivot turns the carries into NaN,
+// which the kernel checks once per tile.
+template <typename F>
+__device__ __forceinline__ void fwd_row_lean(F ds, F dl, F d, F du, F dw, F b,
+                                             Carry<F> &c, F &du2, F &dw2, F &x2) {
+  const F ddl = dl - ds * c.u2;
+  const F dd = d - ds * c.w2 - ddl * c.u1;
+  const F inv = rcp_nr(dd);
+  du2 = (du - ddl * c.w1) * inv;
+  dw2 = dw * inv;
+  x2 = (b - ds * c.y2 - ddl * c.y1) * inv;
+  c.u2 = c.u1; c.u1 = du2;
+  c.w2 = c.w1; c.w1 = dw2;
+  c.y2 = c.y1; c.y1 = x2;
+}
+
+// Warp 0 computes (lanes 0..15: upper halves of 16 systems, 16..31: lower
+// halves); lane 0 of warp 1 is the producer.
+template <typename F, int R, int STAGES, int XST>
+__global__ void __launch_bounds__(64)
+tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
+                   int n, int inner, int tiles_per_run, int n_tiles,
+                   int *__restrict__ status_word) {
+  using G = TmaGeom<F, R, STAGES, XST>;
+  constexpr int SE = G::SE, XE = G::XE;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  F *const ring = reinterpret_cast<F *>(smem_raw);
+  F *const fac = ring + STAGES * SE;          // [n][2][16]: du2, dw2
+  F *const xr = fac + n * 2 * TS;             // [XST][R][32]
+  uint64_t *const full = reinterpret_cast<uint64_t *>(xr + XST * XE);
+  uint64_t *const empty = full + STAGES;
+
+  const int warp = threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  // TMA writes shared memory at 128-byte aligned addresses only; refuse to
+  // run (and report) rather than issue a misaligned copy.
+  if ((smem_u32(smem_raw) & 127u) != 0u) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(status_word, STATUS_TIMEOUT_BIT);
+    return;
+  }
+  const int mt = (n + 1) / 2;
+  const int mb = n - mt;
+  const int n_stages = (mt + R - 1) / R;
+  const int my_first = blockIdx.x;
+  const int my_tiles =
+      (my_first < n_tiles) ? (n_tiles - 1 - my_first) / (int)gridDim.x + 1 : 0;
+  const int total = my_tiles * n_stages;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+
+  // ------------------------------- producer --------------------------------
+  if (warp == 1) {
+    if (lane != 0) return;
+    constexpr unsigned kStageBytes = 12u * R * TS * sizeof(F);
+    // the lower half reads the mirrored band: ds<-dw, dl<-du, d, du<-dl,
+    // dw<-ds, rhs
+    constexpr int kMirror[6] = {4, 3, 2, 1, 0, 5};
+    int slot = 0, use = 0, g = 0, ti = 0;
+    int run = my_first / tiles_per_run;
+    int j0 = (my_first - run * tiles_per_run) * TS;
+    for (int gs = 0; gs < total; ++gs) {
+      if (use > 0 && !mbar_wait(&empty[slot], (unsigned)(use - 1) & 1u)) {
+        atomicOr(status_word, STATUS_TIMEOUT_BIT);
+        return;
+      }
+      F *dst = ring + slot * SE;
+      mbar_expect_tx(&full[slot], kStageBytes);
+      const int r_up = g * R;            // upper half: rows r_up ..
+      const int r_dn = n - (g + 1) * R;  // lower half: rows r_dn ..
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        tma_load_3d(dst + (q * 2 + 0) * R * TS, &maps.m[q], &full[slot], j0, r_up, run);
+        tma_load_3d(dst + (q * 2 + 1) * R * TS, &maps.m[kMirror[q]], &full[slot], j0,
+                    r_dn, run);
+      }
+      if (++slot == STAGES) { slot = 0; ++use; }
+      if (++g == n_stages) {
+        g = 0;
+        if (++ti < my_tiles) {
+          const int tile = my_first + ti * (int)gridDim.x;
+          run = tile / tiles_per_run;
+          j0 = (tile - run * tiles_per_run) * TS;
+        }
+      }
+    }
+    return;
+  }
+
+  // ------------------------------- consumer --------------------------------
+  const int sys = lane % TS;
+  const int part = lane / TS;
+  const int my_rows = part ? mb : mt;
+  const int fstep = part ? -2 * TS : 2 * TS;
+  int slot = 0;
+  unsigned phase = 0;
+  bool bad = false, timed_out = false;
+  for (int ti = 0; ti < my_tiles; ++ti) {
+    const int tile = my_first + ti * (int)gridDim.x;
+    const int run = tile / tiles_per_run;
+    const int j0 = (tile - run * tiles_per_run) * TS;
+    const bool active = j0 + sys < inner;
+    const int xstep = part ? -inner : inner;  // element offset per row
+    int xo = run * inner * n + j0 + sys + (part ? (n - 1) * inner : 0);
+
+    Carry<F> c;
+    c.zero();
+    F *fp = fac + (part ? (n - 1) : 0) * 2 * TS + sys;  // du2 fp[0], dw2 fp[TS]
+    for (int g = 0; g < n_stages; ++g) {
+      if (!mbar_wait(&full[slot], phase)) { timed_out = true; break; }
+      F *v = ring + slot * SE + part * R * TS + sys + (part ? (R - 1) * TS : 0);
+      const int vs = part ? -TS : TS;
+      if (g == 0) {  // couplings that leave the line: ds' rows 0,1, dl' row 0
+        v[0] = F(0);
+        v[vs] = F(0);
+        v[2 * R * TS] = F(0);
+        // order these generic writes before the slot's next TMA refill
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      }
+      if (active) {
+        if (g * R + R <= my_rows) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const F *w = v + r * vs;
+            F u, vv, y;
+            fwd_row_lean(w[0], w[2 * R * TS], w[4 * R * TS], w[6 * R * TS],
+                         w[8 * R * TS], w[10 * R * TS], c, u, vv, y);
+            fp[0] = u;
+            fp[TS] = vv;
+            fp += fstep;
+            x[xo] = y;
+            xo += xstep;
+          }
+        } else {
+          const int rows = my_rows - g * R;
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            if (r < rows) {
+              const F *w = v + r * vs;
+              F u, vv, y;
+              fwd_row_lean(w[0], w[2 * R * TS], w[4 * R * TS], w[6 * R * TS],
+                           w[8 * R * TS], w[10 * R * TS], c, u, vv, y);
+              fp[0] = u;
+              fp[TS] = vv;
+              fp += fstep;
+              x[xo] = y;
+              xo += xstep;
+            }
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[slot]);
+      if (++slot == STAGES) { slot = 0; phase ^= 1u; }
+    }
+    if (timed_out) break;
+    bad |= !(isfinite(c.u1) && isfinite(c.u2) && isfinite(c.w1) &&
+             isfinite(c.w2) && isfinite(c.y1) && isfinite(c.y2));
+
+    // ---- interface ---------------------------------------------------------
+    const F pu1 = __shfl_xor_sync(0xffffffffu, c.u1, TS);
+    const F pu2 = __shfl_xor_sync(0xffffffffu, c.u2, TS);
+    const F pw1 = __shfl_xor_sync(0xffffffffu, c.w1, TS);
+    const F pw2 = __shfl_xor_sync(0xffffffffu, c.w2, TS);
+    const F py1 = __shfl_xor_sync(0xffffffffu, c.y1, TS);
+    const F py2 = __shfl_xor_sync(0xffffffffu, c.y2, TS);
+    F u0, u1, u2, u3;
+    if (part == 0)
+      solve_interface(c.u2, c.w2, c.y2, c.u1, c.w1, c.y1, pu1, pw1, py1, pu2,
+                      pw2, py2, u0, u1, u2, u3);
+    else
+      solve_interface(pu2, pw2, py2, pu1, pw1, py1, c.u1, c.w1, c.y1, c.u2,
+                      c.w2, c.y2, u0, u1, u2, u3);
+    // The solution just beyond this half's last row: x(K+1), x(K+2).
+    F xa = part ? u1 : u2;
+    F xb = part ? u0 : u3;
+
+    // ---- backward over all rows k = K .. 0 ---------------------------------
+    // x2(k) was written in place into x; read it back through a cp.async ring
+    // (each lane reads only what it wrote).
+    __threadfence_block();
+    const int xo_end = xo;                     // one row past row K
+    const F *fb = fp - fstep;                  // factors of row K
+    auto xissue = [&](int s) {
+      if (s < n_stages && active) {
+        F *dst = xr + (s % XST) * XE + lane;
+        int o = xo_end - (1 + s * R) * xstep;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if (s * R + r < my_rows) cp_async_ca<sizeof(F)>(dst + r * 32, x + o);
+          o -= xstep;
+        }
+      }
+      cp_async_commit();
+    };
+    for (int s = 0; s < XST - 1; ++s) xissue(s);
+    int xw = xo_end - xstep;                   // output offset of row K
+    for (int s = 0; s < n_stages; ++s) {
+      xissue(s + XST - 1);
+      cp_async_wait<XST - 1>();
+      if (active) {
+        const F *src = xr + (s % XST) * XE + lane;
+        if (s * R + R <= my_rows) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const F xk = src[r * 32] - fb[0] * xa - fb[TS] * xb;
+            x[xw] = xk;
+            xw -= xstep;
+            fb -= fstep;
+            xb = xa;
+            xa = xk;
+          }
+        } else {
+          const int rows = my_rows - s * R;
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            if (r < rows) {
+              const F xk = src[r * 32] - fb[0] * xa - fb[TS] * xb;
+              x[xw] = xk;
+              xw -= xstep;
+              fb -= fstep;
+              xb = xa;
+              xa = xk;
+            }
+          }
+        }
+      }
+    }
+    cp_async_wait<0>();
+    __syncwarp();
+  }
+
+  if (timed_out) {
+    // give copies that may still be in flight a bounded chance to land
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_wait(&full[slot], phase);
+      if (++slot == STAGES) { slot = 0; phase ^= 1u; }
+    }
+    if (lane == 0) atomicOr(status_word, STATUS_TIMEOUT_BIT);
+    return;
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0)
+    atomicOr(status_word, STATUS_ZERO_PIVOT_BIT);
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault,
+                                &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+template <typename F>
+bool encode_map(CUtensorMap *m, const F *ptr, const Lines &L, int R) {
+  auto fn = encode_fn();
+  if (fn == nullptr) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)L.inner, (cuuint64_t)L.n,
+                              (cuuint64_t)(L.n_sys / L.inner)};
+  const cuuint64_t strides[2] = {(cuuint64_t)L.inner * sizeof(F),
+                                 (cuuint64_t)L.inner * L.n * sizeof(F)};
+  const cuuint32_t box[3] = {(cuuint32_t)TS, (cuuint32_t)R, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = fn(m,
+                  sizeof(F) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                  3, const_cast<F *>(ptr), dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <typename F, int R, int ST, int XST>
+cudaError_t tma_launch(const SolveArgs<F> &a, int grid, cudaStream_t stream) {
+  using G = TmaGeom<F, R, ST, XST>;
+  TmaMaps maps;
+  const F *ptrs[6] = {a.ds, a.dl, a.d, a.du, a.dw, a.x};
+  for (int q = 0; q < 6; ++q)
+    if (!encode_map<F>(&maps.m[q], ptrs[q], a.L, R)) return cudaErrorInvalidValue;
+  auto kern = tma_strided_kernel<F, R, ST, XST>;
+  const size_t smem = G::smem_bytes(a.L.n);
+  cudaError_t err = cudaFuncSetAttribute(
+      kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
+  const int inner = (int)a.L.inner, n = (int)a.L.n;
+  const int tiles_per_run = (inner + TS - 1) / TS;
+  const int n_tiles = (int)(a.L.n_sys / a.L.inner) * tiles_per_run;
+  if (grid <= 0 || grid > n_tiles) grid = n_tiles;
+  kern<<<grid, 64, smem, stream>>>(maps, a.x, n, inner, tiles_per_run, n_tiles,
+                                   a.status);
+  return cudaGetLastError();
+}
+
+template <typename F, int R, int ST, int XST> int tma_occ(long long n) {
+  using G = TmaGeom<F, R, ST, XST>;
+  auto kern = tma_strided_kernel<F, R, ST, XST>;
+  const size_t smem = G::smem_bytes(n);
+  int blocks = 0;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, 64, smem) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return blocks;
+}
+
+}  // namespace
+
+#define PENTA_TMA_CONFIGS(X) \
+  X(double, 8, 3, 4)         \
+  X(double, 4, 4, 6)         \
+  X(double, 8, 2, 4)         \
+  X(float, 8, 3, 4)          \
+  X(float, 8, 4, 4)
+
+template <typename F> const std::vector<TmaConfig> &tma_configs() {
+  static const std::vector<TmaConfig> v = [] {
+    std::vector<TmaConfig> out;
+#define PENTA_X(FT_, R_, ST_, XST_) \
+  if (std::is_same<F, FT_>::value) out.push_back(TmaConfig{R_, ST_, XST_});
+    PENTA_TMA_CONFIGS(PENTA_X)
+#undef PENTA_X
+    return out;
+  }();
+  return v;
+}
+
+template <typename F> size_t tma_smem_bytes(const TmaConfig &c, long long n) {
+  return (size_t)((long long)c.stages * 6 * 2 * c.R * TS + n * 2 * TS +
+                  (long long)c.xstages * c.R * 32) *
+             sizeof(F) +
+         2 * c.stages * sizeof(uint64_t);
+}
+
+template <typename F> int tma_occupancy(const TmaConfig &c, long long n) {
+#define PENTA_X(FT_, R_, ST_, XST_)                                       \
+  if (std::is_same<F, FT_>::value && c.R == R_ && c.stages == ST_ &&      \
+      c.xstages == XST_)                                                  \
+    return tma_occ<FT_, R_, ST_, XST_>(n);
+  PENTA_TMA_CONFIGS(PENTA_X)
+#undef PENTA_X
+  return 0;
+}
+
+template <typename F>
+bool tma_supported(const SolveArgs<F> &a) {
+  if (encode_fn() == nullptr) return false;
+  if (a.L.inner == 1) return false;                        // strided only
+  if ((a.L.inner * sizeof(F)) % 16 != 0) return false;     // row stride
+  if (a.L.n * a.L.n_sys >= (1LL << 31)) return false;
+  if (a.L.inner > 0xffffffffLL || a.L.n_sys / a.L.inner > 0xffffffffLL) return false;
+  const void *ptrs[6] = {a.ds, a.dl, a.d, a.du, a.dw, a.x};
+  for (const void *p : ptrs)
+    if (reinterpret_cast<uintptr_t>(p) % 16 != 0) return false;
+  return true;
+}
+
+template <typename F>
+cudaError_t launch_tma(const SolveArgs<F> &a, const TmaConfig &c, int grid,
+                       cudaStream_t stream) {
+#define PENTA_X(FT_, R_, ST_, XST_)                                       \
+  if (std::is_same<F, FT_>::value && c.R == R_ && c.stages == ST_ &&      \
+      c.xstages == XST_)                                                  \
+    return tma_launch<FT_, R_, ST_, XST_>(                                \
+        reinterpret_cast<const SolveArgs<FT_> &>(a), grid, stream);
+  PENTA_TMA_CONFIGS(PENTA_X)
+#undef PENTA_X
+  return cudaErrorInvalidConfiguration;
+}
+
+template const std::vector<TmaConfig> &tma_configs<double>();
+template const std::vector<TmaConfig> &tma_configs<float>();
+template size_t tma_smem_bytes<double>(const TmaConfig &, long long);
+template size_t tma_smem_bytes<float>(const TmaConfig &, long long);
+template int tma_occupancy<double>(const TmaConfig &, long long);
+template int tma_occupancy<float>(const TmaConfig &, long long);
+template bool tma_supported<double>(const SolveArgs<double> &);
+template bool tma_supported<float>(const SolveArgs<float> &);
+template cudaError_t launch_tma<double>(const SolveArgs<double> &,
+                                        const TmaConfig &, int, cudaStream_t);
+template cudaError_t launch_tma<float>(const SolveArgs<float> &,
+                                       const TmaConfig &, int, cudaStream_t);
+
+}  // namespace penta

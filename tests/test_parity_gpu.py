@@ -255,3 +255,23 @@ def test_256cube_properties(cuda, solvedim):
     solve_dev(dv, solvedim)
     lin = (2 * x_auto + x2).cpu().numpy()
     assert fwd_err(dv["x"].cpu().numpy(), lin) <= 1e-12
+
+
+@pytest.mark.parametrize("dims", [(64, 64, 64), (48, 20, 33), (32, 40, 16)])
+def test_strided_kernels_with_and_without_tma(cuda, dims, monkeypatch):
+    """The TMA-fed strided kernel and the cp.async one agree with the oracle
+    (PENTA_NO_TMA=1 forces the latter on shapes TMA accepts)."""
+    co = fixtures.random_dominant(dims, 55, np.float64)
+    for solvedim in (1, 2):
+        ref = co["x"].copy()
+        oracle.solve(co["ds"], co["dl"], co["d"], co["du"], co["dw"], ref, solvedim)
+        variants = []
+        for no_tma in ("0", "1"):
+            monkeypatch.setenv("PENTA_NO_TMA", no_tma)
+            dv = to_dev(co)
+            with ps.Handle() as h:
+                solve_dev(dv, solvedim, handle=h)
+                variants.append(h.variant_that_ran(direction(3, solvedim)))
+            assert fwd_err(dv["x"].cpu().numpy(), ref) <= 1e-12, (dims, solvedim, no_tma)
+        if dims[0] % 2 == 0:
+            assert "tma" in variants[0] and "tma" not in variants[1], variants
