@@ -127,7 +127,7 @@ __device__ __forceinline__ void fwd_row_lean(F ds, F dl, F d, F du, F dw, F b,
 // Warp 0 computes (lanes 0..15: upper halves of 16 systems, 16..31: lower
 // halves); lane 0 of warp 1 is the producer.
 template <typename F, int R, int STAGES, int XST>
-__global__ void __launch_bounds__(64)
+__global__ void __launch_bounds__(64, 1)
 tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
                    int n, int inner, int tiles_per_run, int n_tiles,
                    int *__restrict__ status_word) {
@@ -233,41 +233,56 @@ tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
         // order these generic writes before the slot's next TMA refill
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       }
-      if (active) {
-        if (g * R + R <= my_rows) {
+      // Whole stage into registers, then hand the slot back to the producer
+      // before computing: no load waits behind a store, and the refill starts
+      // one stage earlier.
+      F a[R][6];
 #pragma unroll
-          for (int r = 0; r < R; ++r) {
-            const F *w = v + r * vs;
-            F u, vv, y;
-            fwd_row_lean(w[0], w[2 * R * TS], w[4 * R * TS], w[6 * R * TS],
-                         w[8 * R * TS], w[10 * R * TS], c, u, vv, y);
-            fp[0] = u;
-            fp[TS] = vv;
-            fp += fstep;
-            x[xo] = y;
-            xo += xstep;
-          }
-        } else {
-          const int rows = my_rows - g * R;
+      for (int r = 0; r < R; ++r)
 #pragma unroll
-          for (int r = 0; r < R; ++r) {
-            if (r < rows) {
-              const F *w = v + r * vs;
-              F u, vv, y;
-              fwd_row_lean(w[0], w[2 * R * TS], w[4 * R * TS], w[6 * R * TS],
-                           w[8 * R * TS], w[10 * R * TS], c, u, vv, y);
-              fp[0] = u;
-              fp[TS] = vv;
-              fp += fstep;
-              x[xo] = y;
-              xo += xstep;
-            }
-          }
-        }
-      }
+        for (int q = 0; q < 6; ++q) a[r][q] = v[r * vs + q * 2 * R * TS];
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[slot]);
       if (++slot == STAGES) { slot = 0; phase ^= 1u; }
+      if (active) {
+        const int rows = min(R, my_rows - g * R);
+        const Carry<F> c0 = c;
+        F u[R], vv[R], y[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          fwd_row_lean(a[r][0], a[r][1], a[r][2], a[r][3], a[r][4], a[r][5], c,
+                       u[r], vv[r], y[r]);
+        if (rows == R) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            fp[r * fstep] = u[r];
+            fp[r * fstep + TS] = vv[r];
+            x[xo + r * xstep] = y[r];
+          }
+          fp += R * fstep;
+          xo += R * xstep;
+        } else {
+          // partial last stage: keep the rows that exist and rebuild the
+          // carries from them (rows past the line were computed on filler)
+          Carry<F> cr = c0;
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            if (r < rows) {
+              fp[r * fstep] = u[r];
+              fp[r * fstep + TS] = vv[r];
+              x[xo + r * xstep] = y[r];
+              cr.u2 = cr.u1; cr.u1 = u[r];
+              cr.w2 = cr.w1; cr.w1 = vv[r];
+              cr.y2 = cr.y1; cr.y1 = y[r];
+            }
+          }
+          c = cr;
+          if (rows > 0) {
+            fp += rows * fstep;
+            xo += rows * xstep;
+          }
+        }
+      }
     }
     if (timed_out) break;
     bad |= !(isfinite(c.u1) && isfinite(c.u2) && isfinite(c.w1) &&
@@ -312,33 +327,34 @@ tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
     for (int s = 0; s < XST - 1; ++s) xissue(s);
     int xw = xo_end - xstep;                   // output offset of row K
     for (int s = 0; s < n_stages; ++s) {
-      xissue(s + XST - 1);
-      cp_async_wait<XST - 1>();
+      cp_async_wait<XST - 2>();                // stage s has landed
+      const F *src = xr + (s % XST) * XE + lane;
+      F xs[R], du[R], dw[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        xs[r] = src[r * 32];
+        du[r] = fb[-r * fstep];
+        dw[r] = fb[-r * fstep + TS];
+      }
+      xissue(s + XST - 1);                     // refills the slot of stage s-1
       if (active) {
-        const F *src = xr + (s % XST) * XE + lane;
-        if (s * R + R <= my_rows) {
+        const int rows = min(R, my_rows - s * R);
+        F xk[R];
 #pragma unroll
-          for (int r = 0; r < R; ++r) {
-            const F xk = src[r * 32] - fb[0] * xa - fb[TS] * xb;
-            x[xw] = xk;
-            xw -= xstep;
-            fb -= fstep;
-            xb = xa;
-            xa = xk;
-          }
+        for (int r = 0; r < R; ++r) {
+          xk[r] = xs[r] - du[r] * xa - dw[r] * xb;
+          xb = xa;
+          xa = xk[r];
+        }
+        if (rows == R) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) x[xw - r * xstep] = xk[r];
+          xw -= R * xstep;
+          fb -= R * fstep;
         } else {
-          const int rows = my_rows - s * R;
 #pragma unroll
-          for (int r = 0; r < R; ++r) {
-            if (r < rows) {
-              const F xk = src[r * 32] - fb[0] * xa - fb[TS] * xb;
-              x[xw] = xk;
-              xw -= xstep;
-              fb -= fstep;
-              xb = xa;
-              xa = xk;
-            }
-          }
+          for (int r = 0; r < R; ++r)
+            if (r < rows) x[xw - r * xstep] = xk[r];
         }
       }
     }
@@ -437,6 +453,7 @@ template <typename F, int R, int ST, int XST> int tma_occ(long long n) {
 }  // namespace
 
 #define PENTA_TMA_CONFIGS(X) \
+  X(double, 8, 3, 6)         \
   X(double, 8, 3, 4)         \
   X(double, 4, 4, 6)         \
   X(double, 8, 2, 4)         \
