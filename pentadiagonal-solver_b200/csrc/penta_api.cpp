@@ -241,12 +241,26 @@ bool pick_tiled(Context &ctx, const Lines &L, bool contig, int P,
 // The TMA-fed strided variant: most resident CTAs (capped at 4), then the
 // deepest ring.
 template <typename F>
-bool pick_tma(Context &ctx, const SolveArgs<F> &a, TmaConfig &out, int &occ_out) {
+bool pick_tma(Context &ctx, const SolveArgs<F> &a, size_t usable_buf, TmaConfig &out,
+              int &occ_out) {
   if (!tma_supported<F>(a)) return false;
+  // the scratch variants keep (dw2, x2) in the caller's buffer
+  const bool scr_ok = a.scratch != nullptr &&
+                      reinterpret_cast<uintptr_t>(a.scratch) % 16 == 0 &&
+                      tma_scratch_bytes<F>(a.L) <= usable_buf;
   const std::vector<TmaConfig> &all = tma_configs<F>();
+  // PENTA_TMA_VARIANT="R,stages,xstages,scratch" restricts the choice (tuning)
+  int want[4] = {-1, -1, -1, -1};
+  if (const char *e = std::getenv("PENTA_TMA_VARIANT"))
+    std::sscanf(e, "%d,%d,%d,%d", &want[0], &want[1], &want[2], &want[3]);
   int best = -1, best_score = -1, best_occ = 0;
   for (size_t i = 0; i < all.size(); ++i) {
     const TmaConfig &c = all[i];
+    if (c.scratch && !scr_ok) continue;
+    if ((want[0] >= 0 && c.R != want[0]) || (want[1] >= 0 && c.stages != want[1]) ||
+        (want[2] >= 0 && c.xstages != want[2]) ||
+        (want[3] >= 0 && (int)c.scratch != want[3]))
+      continue;
     if (tma_smem_bytes<F>(c, a.L.n) > (size_t)ctx.smem_optin) continue;
     int occ;
     const long long key =
@@ -364,12 +378,13 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
       if (!contig && P == 2 && !env_flag("PENTA_NO_TMA")) {
         TmaConfig tc{};
         int occ = 0;
-        if (pick_tma<F>(ctx, a, tc, occ)) {
+        const size_t usable = std::min(buf_bytes, buffer_bytes(sh, sizeof(F)));
+        if (pick_tma<F>(ctx, a, usable, tc, occ)) {
           err = launch_tma<F>(a, tc, occ * ctx.sm_count, stream);
           if (err == cudaSuccess) {
             char buf[96];
-            std::snprintf(buf, sizeof buf, "thomas-pcr:tma P2 S16 R%d x%d/%d",
-                          tc.R, tc.stages, tc.xstages);
+            std::snprintf(buf, sizeof buf, "thomas-pcr:tma P2 S16 R%d x%d/%d%s",
+                          tc.R, tc.stages, tc.xstages, tc.scratch ? " scr" : "");
             record(ctx, dir, "thomas-pcr", buf);
             return PENTAD_STATUS_SUCCESS;
           }

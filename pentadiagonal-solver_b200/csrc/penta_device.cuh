@@ -143,6 +143,14 @@ __device__ __forceinline__ void cp_async_ca(void *dst_smem, const void *src) {
                "l"(src), "n"(BYTES)
                : "memory");
 }
+template <int BYTES>
+__device__ __forceinline__ void cp_async_cg(void *dst_smem, const void *src) {
+  static_assert(BYTES == 16, "cp.async.cg copies 16 bytes");
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                   smem_u32(dst_smem)),
+               "l"(src)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }

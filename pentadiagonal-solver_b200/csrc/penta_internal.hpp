@@ -42,10 +42,17 @@ cudaError_t launch_tiled2(const SolveArgs<F> &a, const TiledConfig &cfg,
 
 // A compiled variant of the TMA-fed strided kernel (tma_kernels.cu).
 struct TmaConfig {
-  int R;        // rows per ring stage
-  int stages;   // ring stages
-  int xstages;  // stages of the x2 read-back ring
+  int R;         // rows per ring stage
+  int stages;    // ring stages
+  int xstages;   // stages of the read-back ring
+  bool scratch;  // (dw2, x2) in the caller's buffer instead of smem / x
 };
+
+// Bytes of caller buffer the scratch variant of the TMA kernel uses.
+template <typename F> inline size_t tma_scratch_bytes(const Lines &L) {
+  const long long tiles = (L.n_sys / L.inner) * ((L.inner + 15) / 16);
+  return (size_t)tiles * (size_t)L.n * 32 * sizeof(F);
+}
 template <typename F> const std::vector<TmaConfig> &tma_configs();
 template <typename F> size_t tma_smem_bytes(const TmaConfig &c, long long n);
 template <typename F> int tma_occupancy(const TmaConfig &c, long long n);

@@ -31,6 +31,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <cstdlib>
 #include <mutex>
 
 #include "penta_device.cuh"
@@ -91,15 +92,25 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map,
       : "memory");
 }
 
-template <typename F, int R, int STAGES, int XST>
+template <typename F> struct Vec2;
+template <> struct Vec2<double> { using T = double2; };
+template <> struct Vec2<float> { using T = float2; };
+
+// SCR = false: du2, dw2 in shared memory, x2 written in place into x.
+// SCR = true:  du2 in shared memory, (dw2, x2) pairs in the caller's scratch
+//              buffer ([tile][row][16 systems][2]), one vector store per row.
+template <typename F, int R, int STAGES, int XST, bool SCR>
 struct TmaGeom {
-  static constexpr int SE = 6 * 2 * R * TS;   // ring stage (elements)
-  static constexpr int XE = R * 32;           // x2 ring stage (elements)
+  static constexpr int SE = 6 * 2 * R * TS;            // ring stage (elements)
+  static constexpr int FW = SCR ? TS : 2 * TS;          // factor row (elements)
+  static constexpr int XE = R * 32 * (SCR ? 2 : 1);     // read-back stage
+  // Rounded up to 1 KB so that every co-resident CTA's window (and with it
+  // each 128-byte aligned TMA destination) starts aligned.
   static size_t smem_bytes(long long n) {
-    // [ring][du2,dw2 interleaved: n x 2 x 16][x2 ring][full, empty barriers]
-    return (size_t)((long long)STAGES * SE + n * 2 * TS + (long long)XST * XE) *
-               sizeof(F) +
-           2 * STAGES * sizeof(uint64_t);
+    const size_t b = (size_t)((long long)STAGES * SE + n * FW + (long long)XST * XE) *
+                         sizeof(F) +
+                     2 * STAGES * sizeof(uint64_t);
+    return (b + 1023) & ~size_t(1023);
   }
 };
 
@@ -126,17 +137,18 @@ __device__ __forceinline__ void fwd_row_lean(F ds, F dl, F d, F du, F dw, F b,
 
 // Warp 0 computes (lanes 0..15: upper halves of 16 systems, 16..31: lower
 // halves); lane 0 of warp 1 is the producer.
-template <typename F, int R, int STAGES, int XST>
+template <typename F, int R, int STAGES, int XST, bool SCR>
 __global__ void __launch_bounds__(64, 1)
 tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
-                   int n, int inner, int tiles_per_run, int n_tiles,
-                   int *__restrict__ status_word) {
-  using G = TmaGeom<F, R, STAGES, XST>;
-  constexpr int SE = G::SE, XE = G::XE;
+                   F *__restrict__ scratch, int n, int inner, int tiles_per_run,
+                   int n_tiles, int *__restrict__ status_word, int dbg) {
+  using G = TmaGeom<F, R, STAGES, XST, SCR>;
+  using V2 = typename Vec2<F>::T;
+  constexpr int SE = G::SE, XE = G::XE, FW = G::FW;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   F *const ring = reinterpret_cast<F *>(smem_raw);
-  F *const fac = ring + STAGES * SE;          // [n][2][16]: du2, dw2
-  F *const xr = fac + n * 2 * TS;             // [XST][R][32]
+  F *const fac = ring + STAGES * SE;          // [n][FW]
+  F *const xr = fac + n * FW;                 // [XST][R][32](x2 or (dw2,x2))
   uint64_t *const full = reinterpret_cast<uint64_t *>(xr + XST * XE);
   uint64_t *const empty = full + STAGES;
 
@@ -207,7 +219,8 @@ tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
   const int sys = lane % TS;
   const int part = lane / TS;
   const int my_rows = part ? mb : mt;
-  const int fstep = part ? -2 * TS : 2 * TS;
+  const int fstep = part ? -FW : FW;       // factor row step (elements)
+  const int sstep = part ? -2 * TS : 2 * TS;  // scratch row step (elements)
   int slot = 0;
   unsigned phase = 0;
   bool bad = false, timed_out = false;
@@ -217,11 +230,15 @@ tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
     const int j0 = (tile - run * tiles_per_run) * TS;
     const bool active = j0 + sys < inner;
     const int xstep = part ? -inner : inner;  // element offset per row
-    int xo = run * inner * n + j0 + sys + (part ? (n - 1) * inner : 0);
+    const int row0 = part ? (n - 1) : 0;       // first row in elimination order
+    int xo = run * inner * n + j0 + sys + row0 * inner;
+    // (dw2, x2) of this lane's rows: [row][16][2] inside the tile's region
+    F *const sg = SCR ? scratch + (long long)tile * n * 2 * TS : nullptr;
+    int so = (row0 * TS + sys) * 2;
 
     Carry<F> c;
     c.zero();
-    F *fp = fac + (part ? (n - 1) : 0) * 2 * TS + sys;  // du2 fp[0], dw2 fp[TS]
+    F *fp = fac + row0 * FW + sys;             // du2 fp[0] (, dw2 fp[TS])
     for (int g = 0; g < n_stages; ++g) {
       if (!mbar_wait(&full[slot], phase)) { timed_out = true; break; }
       F *v = ring + slot * SE + part * R * TS + sys + (part ? (R - 1) * TS : 0);
@@ -241,8 +258,14 @@ tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
       for (int r = 0; r < R; ++r)
 #pragma unroll
         for (int q = 0; q < 6; ++q) a[r][q] = v[r * vs + q * 2 * R * TS];
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[slot]);
+      const int my_slot = slot;
+      if (!(dbg & 1)) {
+        // The refill is an async-proxy write: order these generic-proxy reads
+        // before it, or a refill can land under a load still in flight.
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[my_slot]);
+      }
       if (++slot == STAGES) { slot = 0; phase ^= 1u; }
       if (active) {
         const int rows = min(R, my_rows - g * R);
@@ -252,15 +275,24 @@ tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
         for (int r = 0; r < R; ++r)
           fwd_row_lean(a[r][0], a[r][1], a[r][2], a[r][3], a[r][4], a[r][5], c,
                        u[r], vv[r], y[r]);
-        if (rows == R) {
-#pragma unroll
-          for (int r = 0; r < R; ++r) {
-            fp[r * fstep] = u[r];
+        auto put = [&](int r) {
+          fp[r * fstep] = u[r];
+          if constexpr (SCR) {
+            V2 pv;
+            pv.x = vv[r];
+            pv.y = y[r];
+            *reinterpret_cast<V2 *>(sg + so + r * sstep) = pv;
+          } else {
             fp[r * fstep + TS] = vv[r];
             x[xo + r * xstep] = y[r];
           }
+        };
+        if (rows == R) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) put(r);
           fp += R * fstep;
           xo += R * xstep;
+          so += R * sstep;
         } else {
           // partial last stage: keep the rows that exist and rebuild the
           // carries from them (rows past the line were computed on filler)
@@ -268,9 +300,7 @@ tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             if (r < rows) {
-              fp[r * fstep] = u[r];
-              fp[r * fstep + TS] = vv[r];
-              x[xo + r * xstep] = y[r];
+              put(r);
               cr.u2 = cr.u1; cr.u1 = u[r];
               cr.w2 = cr.w1; cr.w1 = vv[r];
               cr.y2 = cr.y1; cr.y1 = y[r];
@@ -280,8 +310,13 @@ tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
           if (rows > 0) {
             fp += rows * fstep;
             xo += rows * xstep;
+            so += rows * sstep;
           }
         }
+      }
+      if (dbg & 1) {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[my_slot]);
       }
     }
     if (timed_out) break;
@@ -307,19 +342,36 @@ tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
     F xb = part ? u0 : u3;
 
     // ---- backward over all rows k = K .. 0 ---------------------------------
-    // x2(k) was written in place into x; read it back through a cp.async ring
-    // (each lane reads only what it wrote).
+    // x2 (and dw2 when SCR) of row k come back through a cp.async ring; each
+    // lane reads only what it wrote.
     __threadfence_block();
     const int xo_end = xo;                     // one row past row K
+    const int so_end = so;
     const F *fb = fp - fstep;                  // factors of row K
     auto xissue = [&](int s) {
       if (s < n_stages && active) {
-        F *dst = xr + (s % XST) * XE + lane;
-        int o = xo_end - (1 + s * R) * xstep;
+        F *dst = xr + (s % XST) * XE + lane * (SCR ? 2 : 1);
+        if constexpr (SCR) {
+          int o = so_end - (1 + s * R) * sstep;
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-          if (s * R + r < my_rows) cp_async_ca<sizeof(F)>(dst + r * 32, x + o);
-          o -= xstep;
+          for (int r = 0; r < R; ++r) {
+            if (s * R + r < my_rows) {
+              if constexpr (sizeof(F) == 8) {
+                if (dbg & 2) cp_async_cg<16>(dst + r * 64, sg + o);
+                else cp_async_ca<16>(dst + r * 64, sg + o);
+              } else {
+                cp_async_ca<2 * sizeof(F)>(dst + r * 64, sg + o);
+              }
+            }
+            o -= sstep;
+          }
+        } else {
+          int o = xo_end - (1 + s * R) * xstep;
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            if (s * R + r < my_rows) cp_async_ca<sizeof(F)>(dst + r * 32, x + o);
+            o -= xstep;
+          }
         }
       }
       cp_async_commit();
@@ -328,15 +380,42 @@ tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
     int xw = xo_end - xstep;                   // output offset of row K
     for (int s = 0; s < n_stages; ++s) {
       cp_async_wait<XST - 2>();                // stage s has landed
-      const F *src = xr + (s % XST) * XE + lane;
       F xs[R], du[R], dw[R];
+      if constexpr (SCR) {
+        const V2 *src = reinterpret_cast<const V2 *>(xr + (s % XST) * XE) + lane;
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        xs[r] = src[r * 32];
-        du[r] = fb[-r * fstep];
-        dw[r] = fb[-r * fstep + TS];
+        for (int r = 0; r < R; ++r) {
+          const V2 pv = src[r * 32];
+          dw[r] = pv.x;
+          xs[r] = pv.y;
+          du[r] = fb[-r * fstep];
+        }
+      } else {
+        const F *src = xr + (s % XST) * XE + lane;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          xs[r] = src[r * 32];
+          du[r] = fb[-r * fstep];
+          dw[r] = fb[-r * fstep + TS];
+        }
       }
       xissue(s + XST - 1);                     // refills the slot of stage s-1
+      if constexpr (SCR) {
+        // The (dw2, x2) lines of stage s are dead once they sit in shared
+        // memory: drop them from L2 so they are never written back to HBM.
+        // Each lane of a half drops one of the half's 2 x R lines; a line
+        // holds 8 lanes' values, so every lane's copy must have landed first.
+        __syncwarp();
+        if (!(dbg & 4) && active) {
+          const int r = sys >> 1, h = sys & 1;
+          const int k = s * R + r;             // k-th row back from row K
+          if (k < my_rows) {
+            const int row = part ? (mt + k) : (mt - 1 - k);
+            const F *line = sg + (row * TS + 8 * h) * 2;
+            asm volatile("discard.global.L2 [%0], 128;\n" ::"l"(line) : "memory");
+          }
+        }
+      }
       if (active) {
         const int rows = min(R, my_rows - s * R);
         F xk[R];
@@ -414,14 +493,14 @@ bool encode_map(CUtensorMap *m, const F *ptr, const Lines &L, int R) {
   return r == CUDA_SUCCESS;
 }
 
-template <typename F, int R, int ST, int XST>
+template <typename F, int R, int ST, int XST, bool SCR>
 cudaError_t tma_launch(const SolveArgs<F> &a, int grid, cudaStream_t stream) {
-  using G = TmaGeom<F, R, ST, XST>;
+  using G = TmaGeom<F, R, ST, XST, SCR>;
   TmaMaps maps;
   const F *ptrs[6] = {a.ds, a.dl, a.d, a.du, a.dw, a.x};
   for (int q = 0; q < 6; ++q)
     if (!encode_map<F>(&maps.m[q], ptrs[q], a.L, R)) return cudaErrorInvalidValue;
-  auto kern = tma_strided_kernel<F, R, ST, XST>;
+  auto kern = tma_strided_kernel<F, R, ST, XST, SCR>;
   const size_t smem = G::smem_bytes(a.L.n);
   cudaError_t err = cudaFuncSetAttribute(
       kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -430,14 +509,16 @@ cudaError_t tma_launch(const SolveArgs<F> &a, int grid, cudaStream_t stream) {
   const int tiles_per_run = (inner + TS - 1) / TS;
   const int n_tiles = (int)(a.L.n_sys / a.L.inner) * tiles_per_run;
   if (grid <= 0 || grid > n_tiles) grid = n_tiles;
-  kern<<<grid, 64, smem, stream>>>(maps, a.x, n, inner, tiles_per_run, n_tiles,
-                                   a.status);
+  int dbg = 0;
+  if (const char *e = std::getenv("PENTA_TMA_DEBUG")) dbg = std::atoi(e);
+  kern<<<grid, 64, smem, stream>>>(maps, a.x, static_cast<F *>(a.scratch), n,
+                                   inner, tiles_per_run, n_tiles, a.status, dbg);
   return cudaGetLastError();
 }
 
-template <typename F, int R, int ST, int XST> int tma_occ(long long n) {
-  using G = TmaGeom<F, R, ST, XST>;
-  auto kern = tma_strided_kernel<F, R, ST, XST>;
+template <typename F, int R, int ST, int XST, bool SCR> int tma_occ(long long n) {
+  using G = TmaGeom<F, R, ST, XST, SCR>;
+  auto kern = tma_strided_kernel<F, R, ST, XST, SCR>;
   const size_t smem = G::smem_bytes(n);
   int blocks = 0;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -453,18 +534,19 @@ template <typename F, int R, int ST, int XST> int tma_occ(long long n) {
 }  // namespace
 
 #define PENTA_TMA_CONFIGS(X) \
-  X(double, 8, 3, 6)         \
-  X(double, 8, 3, 4)         \
-  X(double, 4, 4, 6)         \
-  X(double, 8, 2, 4)         \
-  X(float, 8, 3, 4)          \
-  X(float, 8, 4, 4)
+  X(double, 8, 3, 6, false)  \
+  X(double, 8, 2, 4, true)   \
+  X(double, 8, 3, 4, true)   \
+  X(double, 4, 4, 6, true)   \
+  X(float, 8, 3, 4, false)   \
+  X(float, 8, 3, 4, true)    \
+  X(float, 8, 4, 6, true)
 
 template <typename F> const std::vector<TmaConfig> &tma_configs() {
   static const std::vector<TmaConfig> v = [] {
     std::vector<TmaConfig> out;
-#define PENTA_X(FT_, R_, ST_, XST_) \
-  if (std::is_same<F, FT_>::value) out.push_back(TmaConfig{R_, ST_, XST_});
+#define PENTA_X(FT_, R_, ST_, XST_, SCR_) \
+  if (std::is_same<F, FT_>::value) out.push_back(TmaConfig{R_, ST_, XST_, SCR_});
     PENTA_TMA_CONFIGS(PENTA_X)
 #undef PENTA_X
     return out;
@@ -473,17 +555,20 @@ template <typename F> const std::vector<TmaConfig> &tma_configs() {
 }
 
 template <typename F> size_t tma_smem_bytes(const TmaConfig &c, long long n) {
-  return (size_t)((long long)c.stages * 6 * 2 * c.R * TS + n * 2 * TS +
-                  (long long)c.xstages * c.R * 32) *
-             sizeof(F) +
-         2 * c.stages * sizeof(uint64_t);
+  const long long fw = c.scratch ? TS : 2 * TS;
+  const long long xe = (long long)c.R * 32 * (c.scratch ? 2 : 1);
+  const size_t b = (size_t)((long long)c.stages * 6 * 2 * c.R * TS + n * fw +
+                            (long long)c.xstages * xe) *
+                       sizeof(F) +
+                   2 * c.stages * sizeof(uint64_t);
+  return (b + 1023) & ~size_t(1023);
 }
 
 template <typename F> int tma_occupancy(const TmaConfig &c, long long n) {
-#define PENTA_X(FT_, R_, ST_, XST_)                                       \
+#define PENTA_X(FT_, R_, ST_, XST_, SCR_)                                 \
   if (std::is_same<F, FT_>::value && c.R == R_ && c.stages == ST_ &&      \
-      c.xstages == XST_)                                                  \
-    return tma_occ<FT_, R_, ST_, XST_>(n);
+      c.xstages == XST_ && c.scratch == SCR_)                             \
+    return tma_occ<FT_, R_, ST_, XST_, SCR_>(n);
   PENTA_TMA_CONFIGS(PENTA_X)
 #undef PENTA_X
   return 0;
@@ -505,10 +590,10 @@ bool tma_supported(const SolveArgs<F> &a) {
 template <typename F>
 cudaError_t launch_tma(const SolveArgs<F> &a, const TmaConfig &c, int grid,
                        cudaStream_t stream) {
-#define PENTA_X(FT_, R_, ST_, XST_)                                       \
+#define PENTA_X(FT_, R_, ST_, XST_, SCR_)                                 \
   if (std::is_same<F, FT_>::value && c.R == R_ && c.stages == ST_ &&      \
-      c.xstages == XST_)                                                  \
-    return tma_launch<FT_, R_, ST_, XST_>(                                \
+      c.xstages == XST_ && c.scratch == SCR_)                             \
+    return tma_launch<FT_, R_, ST_, XST_, SCR_>(                          \
         reinterpret_cast<const SolveArgs<FT_> &>(a), grid, stream);
   PENTA_TMA_CONFIGS(PENTA_X)
 #undef PENTA_X

@@ -31,15 +31,19 @@ def direction(ndim: int, solvedim: int) -> int:
     return 2 if solvedim == ndim - 1 else 1
 
 
-def solve_dev(dv: dict, solvedim: int, dims=None, handle=None, buffer=None, stream=None):
-    import torch
-
+def solve_dev(dv: dict, solvedim: int, dims=None, handle=None, buffer=None, stream=None,
+              check_status: bool = True):
+    """Solve through the C ABI; by default also require a clean device status
+    word afterwards (no zero pivot, no timed-out wait, no refused launch)."""
     x = dv["x"]
     dims = ps.dims_of(x) if dims is None else list(dims)
     if buffer is None:
         buffer = ps.alloc_buffer(dims, solvedim, x.dtype, x.device)
     ps.gpsv_batch(dv["ds"], dv["dl"], dv["d"], dv["du"], dv["dw"], x, solvedim,
                   buffer=buffer, handle=handle, dims=dims, stream=stream)
+    if check_status:
+        st, bits = ps.status_check(stream=stream)
+        assert bits == 0, f"device status bits {bits:#x} after solve along {solvedim}"
     return buffer
 
 
