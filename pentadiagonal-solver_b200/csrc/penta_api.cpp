@@ -245,8 +245,9 @@ bool pick_tma(Context &ctx, const SolveArgs<F> &a, size_t usable_buf, TmaConfig 
               int &occ_out) {
   if (!tma_supported<F>(a)) return false;
   // the scratch variants keep (dw2, x2) in the caller's buffer
+  // (128-byte aligned: they drop whole 128-byte lines of it from L2)
   const bool scr_ok = a.scratch != nullptr &&
-                      reinterpret_cast<uintptr_t>(a.scratch) % 16 == 0 &&
+                      reinterpret_cast<uintptr_t>(a.scratch) % 128 == 0 &&
                       tma_scratch_bytes<F>(a.L) <= usable_buf;
   const std::vector<TmaConfig> &all = tma_configs<F>();
   // PENTA_TMA_VARIANT="R,stages,xstages,scratch" restricts the choice (tuning)
@@ -277,6 +278,45 @@ bool pick_tma(Context &ctx, const SolveArgs<F> &a, size_t usable_buf, TmaConfig 
     }
     if (occ <= 0) continue;
     const int score = std::min(occ, 4) * 1000 + c.stages * c.R;
+    if (score > best_score) {
+      best_score = score;
+      best = (int)i;
+      best_occ = occ;
+    }
+  }
+  if (best < 0) return false;
+  out = all[best];
+  occ_out = best_occ;
+  return true;
+}
+
+// The TMA-fed contiguous (x) variant: most resident CTAs (capped at 4), then
+// the deepest ring.  It needs the caller's buffer for (dw2, x2).
+template <typename F>
+bool pick_tma_contig(Context &ctx, const SolveArgs<F> &a, size_t usable_buf,
+                     TmaConfig &out, int &occ_out) {
+  if (!tma_contig_supported<F>(a) || tma_contig_scratch_bytes<F>(a.L) > usable_buf)
+    return false;
+  const std::vector<TmaConfig> &all = tma_contig_configs<F>();
+  int best = -1, best_score = -1, best_occ = 0;
+  for (size_t i = 0; i < all.size(); ++i) {
+    const TmaConfig &c = all[i];
+    if (tma_contig_smem_bytes<F>(c, a.L.n) > (size_t)ctx.smem_optin) continue;
+    int occ;
+    const long long key =
+        (1LL << 61) | ((long long)i << 40) | (a.L.n << 1) | (sizeof(F) == 8);
+    {
+      std::lock_guard<std::mutex> lock(ctx.mu);
+      auto it = ctx.occ_cache.find(key);
+      occ = (it != ctx.occ_cache.end()) ? it->second : -1;
+    }
+    if (occ < 0) {
+      occ = tma_contig_occupancy<F>(c, a.L.n);
+      std::lock_guard<std::mutex> lock(ctx.mu);
+      ctx.occ_cache[key] = occ;
+    }
+    if (occ <= 0) continue;
+    const int score = std::min(occ, 4) * 1000 + c.stages;
     if (score > best_score) {
       best_score = score;
       best = (int)i;
@@ -375,6 +415,25 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
     case Algo::Auto:
     default: {
       const int P = (lanes == 1) ? 1 : 2;
+      if (contig && P == 2 && !env_flag("PENTA_NO_TMA")) {
+        TmaConfig tc{};
+        int occ = 0;
+        const size_t usable = std::min(buf_bytes, buffer_bytes(sh, sizeof(F)));
+        if (pick_tma_contig<F>(ctx, a, usable, tc, occ)) {
+          err = launch_tma_contig<F>(a, tc, occ * ctx.sm_count, stream);
+          if (err == cudaSuccess) {
+            char buf[96];
+            std::snprintf(buf, sizeof buf, "thomas-pcr:tma P2 S16 R%d x%d/%d contig",
+                          tc.R, tc.stages, tc.xstages);
+            record(ctx, dir, "thomas-pcr", buf);
+            return PENTAD_STATUS_SUCCESS;
+          }
+          if (debug)
+            std::fprintf(stderr, "[penta] tma launch declined: %s -- falling back\n",
+                         cudaGetErrorString(err));
+          cudaGetLastError();
+        }
+      }
       if (!contig && P == 2 && !env_flag("PENTA_NO_TMA")) {
         TmaConfig tc{};
         int occ = 0;

@@ -61,6 +61,19 @@ template <typename F>
 cudaError_t launch_tma(const SolveArgs<F> &a, const TmaConfig &c, int grid,
                        cudaStream_t stream);
 
+// The TMA-fed contiguous (x) kernel (always keeps (dw2, x2) in the buffer).
+template <typename F> const std::vector<TmaConfig> &tma_contig_configs();
+template <typename F> size_t tma_contig_smem_bytes(const TmaConfig &c, long long n);
+template <typename F> int tma_contig_occupancy(const TmaConfig &c, long long n);
+template <typename F> bool tma_contig_supported(const SolveArgs<F> &a);
+template <typename F>
+cudaError_t launch_tma_contig(const SolveArgs<F> &a, const TmaConfig &c, int grid,
+                              cudaStream_t stream);
+// Bytes of caller buffer the contiguous TMA kernel uses.
+template <typename F> inline size_t tma_contig_scratch_bytes(const Lines &L) {
+  return (size_t)((L.n_sys + 15) / 16) * (size_t)L.n * 32 * sizeof(F);
+}
+
 // penta_status.cu: address of the device status word of `device` (the
 // current device when the address is first taken).
 int *device_status_word(int device);

@@ -285,3 +285,43 @@ def test_strided_kernels_with_and_without_tma(cuda, dims, monkeypatch):
         assert fwd_err(dv["x"].cpu().numpy(), ref) <= 1e-12, (dims, solvedim, var)
         if dims[0] % 2 == 0:
             assert "tma" in var and "scr" not in var, var
+
+
+@pytest.mark.parametrize("dims", [(64, 64, 64), (48, 20, 33), (34, 17, 9), (40, 21, 5),
+                                  (256, 3, 2), (6, 40, 7)])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_contiguous_kernels_with_and_without_tma(cuda, dims, dtype, monkeypatch):
+    """Along x the TMA-fed kernel (rows of 64 bytes, needs n * elem % 16 == 0
+    and a 128-byte aligned buffer) and the cp.async one agree with the oracle;
+    shapes or buffers it does not accept fall back to the cp.async kernel."""
+    import torch
+
+    co = fixtures.random_dominant(dims, 56, dtype)
+    ref = {k: co[k].astype(np.float64) for k in NAMES}
+    oracle.solve(ref["ds"], ref["dl"], ref["d"], ref["du"], ref["dw"], ref["x"], 0)
+    tol = FWD_TOL[dtype]
+    eb = np.dtype(dtype).itemsize
+    n, n_sys = dims[0], int(np.prod(dims[1:]))
+    # it keeps (dw2, x2) for whole tiles of 16 lines in the caller's buffer
+    tma_ok = (n * eb) % 16 == 0 and \
+        -(-n_sys // 16) * n * 32 * eb <= ps.buffer_size(dims, 0, eb)
+    variants = []
+    for no_tma in ("0", "1"):
+        monkeypatch.setenv("PENTA_NO_TMA", no_tma)
+        dv = to_dev(co)
+        with ps.Handle() as h:
+            solve_dev(dv, 0, handle=h)
+            variants.append(h.variant_that_ran(0))
+        assert fwd_err(dv["x"].cpu().numpy(), ref["x"]) <= tol, (dims, no_tma, variants)
+    assert ("tma" in variants[0]) == tma_ok and "tma" not in variants[1], variants
+    # a buffer that is 16- but not 128-byte aligned: the cp.async kernel runs
+    monkeypatch.setenv("PENTA_NO_TMA", "0")
+    dv = to_dev(co)
+    need = ps.buffer_size(dims, 0, np.dtype(dtype).itemsize)
+    raw = torch.empty(need + 256, dtype=torch.uint8, device="cuda")
+    with ps.Handle() as h:
+        ps.gpsv_batch(*(dv[k] for k in NAMES), 0, buffer=raw[16:16 + need], handle=h)
+        var = h.variant_that_ran(0)
+    assert ps.status_check()[1] == 0
+    assert "tma" not in var, var
+    assert fwd_err(dv["x"].cpu().numpy(), ref["x"]) <= tol, (dims, var)
