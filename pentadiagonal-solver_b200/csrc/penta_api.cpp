@@ -158,11 +158,13 @@ pentadStatus_t make_shape(const int *dims, int ndim, int solvedim, Shape &sh,
   return PENTAD_STATUS_SUCCESS;
 }
 
-size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
-
-// Caller buffer layout: [global-scratch Thomas: 3 n n_sys elements].
+// The reference's sizing (src/cuda/singlenode/pentad_cuda.cu:1554-1577): 9 n
+// n_sys elements along x (room for its transpose path), 3 n n_sys otherwise.
+// Every kernel here fits in that: the global-scratch Thomas kernel uses the
+// first 3 n n_sys elements, the on-chip kernels less.
 size_t buffer_bytes(const Shape &sh, size_t elem) {
-  return align256((size_t)3 * (size_t)sh.L.n * (size_t)sh.L.n_sys * elem);
+  const size_t regions = (sh.dir == 0) ? 9 : 3;
+  return regions * (size_t)sh.L.n * (size_t)sh.L.n_sys * elem;
 }
 
 // ---------------------------------------------------------------------------

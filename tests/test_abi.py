@@ -66,7 +66,9 @@ def test_buffer_size_covers_global_scratch(dims, solvedim, elem):
     for v in dims:
         n_total *= v
     b = ps.buffer_size(list(dims), solvedim, elem)
-    assert b >= 3 * n_total * elem
+    # the reference's values (src/cuda/singlenode/pentad_cuda.cu:1554-1577):
+    # 9 n n_sys elements along x (its transpose path), 3 n n_sys otherwise
+    assert b == (9 if solvedim == 0 else 3) * n_total * elem
     # the reference-named sizing functions agree
     fn = getattr(ps.lib(), f"pentadsolver_{'D' if elem == 8 else 'S'}_gpsv_batch_buffer_size_ext")
     assert fn(None, None, None, None, None, None, None, ps._dims(dims), len(dims), solvedim) == b
