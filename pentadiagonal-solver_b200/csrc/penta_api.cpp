@@ -331,6 +331,43 @@ bool pick_tma_contig(Context &ctx, const SolveArgs<F> &a, size_t usable_buf,
   return true;
 }
 
+// The Tensor-Memory kernel: the first compiled variant of this precision and
+// layout that fits shared memory and runs one CTA per SM.
+// PENTA_TMEM_VARIANT="stages,xstages" restricts the choice (tuning).
+template <typename F>
+bool pick_tmem(Context &ctx, const SolveArgs<F> &a, bool contig, size_t usable_buf,
+               TmemConfig &out) {
+  if (!tmem_supported<F>(a, contig, usable_buf)) return false;
+  int want[2] = {-1, -1};
+  if (const char *e = std::getenv("PENTA_TMEM_VARIANT"))
+    std::sscanf(e, "%d,%d", &want[0], &want[1]);
+  const std::vector<TmemConfig> &all = tmem_configs<F>();
+  for (size_t i = 0; i < all.size(); ++i) {
+    const TmemConfig &c = all[i];
+    if (c.contig != contig) continue;
+    if ((want[0] >= 0 && c.stages != want[0]) || (want[1] >= 0 && c.xstages != want[1]))
+      continue;
+    if (c.smem > (size_t)ctx.smem_optin) continue;
+    int occ;
+    const long long key = (1LL << 59) | ((long long)i << 1) | (sizeof(F) == 8);
+    {
+      std::lock_guard<std::mutex> lock(ctx.mu);
+      auto it = ctx.occ_cache.find(key);
+      occ = (it != ctx.occ_cache.end()) ? it->second : -1;
+    }
+    if (occ < 0) {
+      occ = tmem_occupancy<F>(c);
+      std::lock_guard<std::mutex> lock(ctx.mu);
+      ctx.occ_cache[key] = occ;
+    }
+    if (occ == 1) {  // exactly one CTA per SM: it owns all of Tensor Memory
+      out = c;
+      return true;
+    }
+  }
+  return false;
+}
+
 std::string tiled_variant_name(const TiledConfig &c) {
   char buf[96];
   std::snprintf(buf, sizeof buf, "thomas-pcr:tiled P%d S%d R%d x%d%s", c.P,
@@ -417,6 +454,24 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
     case Algo::Auto:
     default: {
       const int P = (lanes == 1) ? 1 : 2;
+      if (P == 2 && !env_flag("PENTA_NO_TMA") && !env_flag("PENTA_NO_TMEM")) {
+        TmemConfig mc{};
+        const size_t usable = std::min(buf_bytes, buffer_bytes(sh, sizeof(F)));
+        if (pick_tmem<F>(ctx, a, contig, usable, mc)) {
+          err = launch_tmem<F>(a, mc, ctx.sm_count, stream);
+          if (err == cudaSuccess) {
+            char vb[96];
+            std::snprintf(vb, sizeof vb, "thomas-pcr:tmem P2 S16 R%d x%d/%d%s", mc.R,
+                          mc.stages, mc.xstages, contig ? " contig" : "");
+            record(ctx, dir, "thomas-pcr", vb);
+            return PENTAD_STATUS_SUCCESS;
+          }
+          if (debug)
+            std::fprintf(stderr, "[penta] tmem launch declined: %s -- falling back\n",
+                         cudaGetErrorString(err));
+          cudaGetLastError();
+        }
+      }
       if (contig && P == 2 && !env_flag("PENTA_NO_TMA")) {
         TmaConfig tc{};
         int occ = 0;

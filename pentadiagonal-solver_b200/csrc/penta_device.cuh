@@ -73,6 +73,23 @@ __device__ __forceinline__ void fwd_row_fast(F ds, F dl, F d, F du, F dw, F b,
   c.y2 = c.y1; c.y1 = x2;
 }
 
+// One row of forward elimination (couplings already masked); as fwd_row_fast
+// without the per-row pivot check -- a zero pivot turns the carries into NaN,
+// which the kernel checks once per tile.
+template <typename F>
+__device__ __forceinline__ void fwd_row_lean(F ds, F dl, F d, F du, F dw, F b,
+                                             Carry<F> &c, F &du2, F &dw2, F &x2) {
+  const F ddl = dl - ds * c.u2;
+  const F dd = d - ds * c.w2 - ddl * c.u1;
+  const F inv = rcp_nr(dd);
+  du2 = (du - ddl * c.w1) * inv;
+  dw2 = dw * inv;
+  x2 = (b - ds * c.y2 - ddl * c.y1) * inv;
+  c.u2 = c.u1; c.u1 = du2;
+  c.w2 = c.w1; c.w1 = dw2;
+  c.y2 = c.y1; c.y1 = x2;
+}
+
 // Zero the out-of-range couplings of row i of an n-row system.
 template <typename F>
 __device__ __forceinline__ void mask_row(long long i, long long n, F &ds,

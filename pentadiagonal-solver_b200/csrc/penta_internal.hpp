@@ -74,6 +74,25 @@ template <typename F> inline size_t tma_contig_scratch_bytes(const Lines &L) {
   return (size_t)((L.n_sys + 15) / 16) * (size_t)L.n * 32 * sizeof(F);
 }
 
+// tmem_kernels.cu: the Thomas kernel with its factors in Tensor Memory (all
+// directions; n <= 256 in FP64, n <= 512 in FP32; x2 goes through the
+// caller's buffer).
+struct TmemConfig {
+  bool contig;   // along x (rows contiguous) or strided
+  int stages;    // forward ring stages per consumer warp
+  int xstages;   // x2 read-back stages per consumer warp
+  int R;         // rows per stage
+  size_t smem;   // dynamic shared memory per CTA
+};
+template <typename F> const std::vector<TmemConfig> &tmem_configs();
+template <typename F> int tmem_occupancy(const TmemConfig &c);
+template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig);
+template <typename F>
+bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf);
+template <typename F>
+cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count,
+                        cudaStream_t stream);
+
 // penta_status.cu: address of the device status word of `device` (the
 // current device when the address is first taken).
 int *device_status_word(int device);

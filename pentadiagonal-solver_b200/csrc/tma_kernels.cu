@@ -28,73 +28,16 @@
 // 16 and a 16-byte aligned innermost coordinate (the system offset is a
 // multiple of 16); the host checks all three and otherwise uses the cp.async
 // kernel.  Rows outside [0, n) read as zeros (never consumed).
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
 #include <cstdlib>
-#include <mutex>
 
-#include "penta_device.cuh"
 #include "penta_internal.hpp"
+#include "tma_device.cuh"
 
 namespace penta {
 namespace {
 
 constexpr int TS = 16;                 // systems per warp
 
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)),
-               "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
-  asm volatile(
-      "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
-          smem_u32(bar)),
-      "r"(bytes)
-      : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-  return t;
-}
-// Bounded wait: false when the barrier did not complete within ~2 s.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const unsigned long long t0 = global_ns();
-  while (!mbar_try_wait(bar, parity))
-    if (global_ns() - t0 > 2000000000ull) return false;
-  return true;
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar))
-               : "memory");
-}
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map,
-                                            uint64_t *bar, int c0, int c1,
-                                            int c2) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2),
-      "r"(smem_u32(bar))
-      : "memory");
-}
-
-template <typename F> struct Vec2;
-template <> struct Vec2<double> { using T = double2; };
-template <> struct Vec2<float> { using T = float2; };
 
 // SCR = false: du2, dw2 in shared memory, x2 written in place into x.
 // SCR = true:  du2 in shared memory, (dw2, x2) pairs in the caller's scratch
@@ -114,26 +57,6 @@ struct TmaGeom {
   }
 };
 
-struct TmaMaps {
-  CUtensorMap m[6];  // ds, dl, d, du, dw, x
-};
-
-// One row of forward elimination (couplings already masked); as fwd_row_fast
-// without the per-row pivot check -- a zero pivot turns the carries into NaN,
-// which the kernel checks once per tile.
-template <typename F>
-__device__ __forceinline__ void fwd_row_lean(F ds, F dl, F d, F du, F dw, F b,
-                                             Carry<F> &c, F &du2, F &dw2, F &x2) {
-  const F ddl = dl - ds * c.u2;
-  const F dd = d - ds * c.w2 - ddl * c.u1;
-  const F inv = rcp_nr(dd);
-  du2 = (du - ddl * c.w1) * inv;
-  dw2 = dw * inv;
-  x2 = (b - ds * c.y2 - ddl * c.y1) * inv;
-  c.u2 = c.u1; c.u1 = du2;
-  c.w2 = c.w1; c.w1 = dw2;
-  c.y2 = c.y1; c.y1 = x2;
-}
 
 // Warp 0 computes (lanes 0..15: upper halves of 16 systems, 16..31: lower
 // halves); lane 0 of warp 1 is the producer.
@@ -485,14 +408,6 @@ struct TmaContigGeom {
   }
 };
 
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map,
-                                            uint64_t *bar, int c0, int c1) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3}], [%4];\n" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
-      : "memory");
-}
 
 template <typename F, int STAGES, int XST>
 __global__ void __launch_bounds__(64, 1)
@@ -746,21 +661,7 @@ tma_contig_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault,
-                                &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    else
-      cudaGetLastError();
-  });
-  return fn;
-}
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() { return tensor_map_encoder(); }
 
 template <typename F>
 bool encode_map(CUtensorMap *m, const F *ptr, const Lines &L, int R) {

@@ -257,71 +257,95 @@ def test_256cube_properties(cuda, solvedim):
     assert fwd_err(dv["x"].cpu().numpy(), lin) <= 1e-12
 
 
-@pytest.mark.parametrize("dims", [(64, 64, 64), (48, 20, 33), (32, 40, 16)])
-def test_strided_kernels_with_and_without_tma(cuda, dims, monkeypatch):
-    """The TMA-fed strided kernel and the cp.async one agree with the oracle
-    (PENTA_NO_TMA=1 forces the latter on shapes TMA accepts)."""
-    co = fixtures.random_dominant(dims, 55, np.float64)
-    for solvedim in (1, 2):
-        ref = co["x"].copy()
-        oracle.solve(co["ds"], co["dl"], co["d"], co["du"], co["dw"], ref, solvedim)
-        variants = []
-        for no_tma in ("0", "1"):
-            monkeypatch.setenv("PENTA_NO_TMA", no_tma)
-            dv = to_dev(co)
-            with ps.Handle() as h:
-                solve_dev(dv, solvedim, handle=h)
-                variants.append(h.variant_that_ran(direction(3, solvedim)))
-            assert fwd_err(dv["x"].cpu().numpy(), ref) <= 1e-12, (dims, solvedim, no_tma)
-        if dims[0] % 2 == 0:
-            assert "tma" in variants[0] and "tma" not in variants[1], variants
-        # without a caller buffer the TMA kernel keeps its factors on chip
-        monkeypatch.setenv("PENTA_NO_TMA", "0")
-        dv = to_dev(co)
-        with ps.Handle() as h:
-            ps.gpsv_batch(*(dv[k] for k in NAMES), solvedim, buffer=None, handle=h)
-            var = h.variant_that_ran(direction(3, solvedim))
-        assert ps.status_check()[1] == 0
-        assert fwd_err(dv["x"].cpu().numpy(), ref) <= 1e-12, (dims, solvedim, var)
-        if dims[0] % 2 == 0:
-            assert "tma" in var and "scr" not in var, var
+def _tmem_ok(dims, solvedim, eb):
+    """Shapes the Tensor-Memory kernel takes: 16-byte aligned rows (x) or runs
+    (y, z), two real rows in each half of the split m = R ceil(n / 2R), at most
+    16 R rows per half (512 TMEM columns), and x2 scratch for whole tiles of 16
+    systems within the reference-sized buffer."""
+    n = dims[solvedim]
+    inner = int(np.prod(dims[:solvedim]))
+    n_sys = int(np.prod(dims)) // n
+    contig = solvedim == 0
+    r = 64 // eb if contig else 1024 // (16 * eb)
+    aligned = (n * eb) % 16 == 0 if contig else (inner > 1 and (inner * eb) % 16 == 0)
+    mt = r * (-(-n // (2 * r)))
+    tiles = -(-n_sys // 16) if contig else (n_sys // inner) * -(-inner // 16)
+    buf = ps.buffer_size(list(dims), solvedim, eb)
+    return aligned and n - mt >= 2 and mt // r <= 16 and tiles * 2 * mt * 16 * eb <= buf
 
 
-@pytest.mark.parametrize("dims", [(64, 64, 64), (48, 20, 33), (34, 17, 9), (40, 21, 5),
-                                  (256, 3, 2), (6, 40, 7)])
-@pytest.mark.parametrize("dtype", [np.float64, np.float32])
-def test_contiguous_kernels_with_and_without_tma(cuda, dims, dtype, monkeypatch):
-    """Along x the TMA-fed kernel (rows of 64 bytes, needs n * elem % 16 == 0
-    and a 128-byte aligned buffer) and the cp.async one agree with the oracle;
-    shapes or buffers it does not accept fall back to the cp.async kernel."""
+def _old_tma_ok(dims, solvedim, eb, buffer=True):
+    """Shapes the older TMA kernels take (without TMEM)."""
+    n = dims[solvedim]
+    inner = int(np.prod(dims[:solvedim]))
+    n_sys = int(np.prod(dims)) // n
+    if solvedim == 0:   # needs its (dw2, x2) scratch in a 128-byte aligned buffer
+        return buffer and (n * eb) % 16 == 0 and \
+            -(-n_sys // 16) * n * 32 * eb <= ps.buffer_size(list(dims), 0, eb)
+    return inner > 1 and (inner * eb) % 16 == 0
+
+
+def _run_chain(co, solvedim, dims, env, monkeypatch, offset=None, buffer=True):
+    """One solve under the given kernel switches; returns (x, variant)."""
     import torch
 
-    co = fixtures.random_dominant(dims, 56, dtype)
-    ref = {k: co[k].astype(np.float64) for k in NAMES}
-    oracle.solve(ref["ds"], ref["dl"], ref["d"], ref["du"], ref["dw"], ref["x"], 0)
-    tol = FWD_TOL[dtype]
-    eb = np.dtype(dtype).itemsize
-    n, n_sys = dims[0], int(np.prod(dims[1:]))
-    # it keeps (dw2, x2) for whole tiles of 16 lines in the caller's buffer
-    tma_ok = (n * eb) % 16 == 0 and \
-        -(-n_sys // 16) * n * 32 * eb <= ps.buffer_size(dims, 0, eb)
-    variants = []
-    for no_tma in ("0", "1"):
-        monkeypatch.setenv("PENTA_NO_TMA", no_tma)
-        dv = to_dev(co)
-        with ps.Handle() as h:
-            solve_dev(dv, 0, handle=h)
-            variants.append(h.variant_that_ran(0))
-        assert fwd_err(dv["x"].cpu().numpy(), ref["x"]) <= tol, (dims, no_tma, variants)
-    assert ("tma" in variants[0]) == tma_ok and "tma" not in variants[1], variants
-    # a buffer that is 16- but not 128-byte aligned: the cp.async kernel runs
-    monkeypatch.setenv("PENTA_NO_TMA", "0")
+    for k in ("PENTA_NO_TMA", "PENTA_NO_TMEM"):
+        monkeypatch.setenv(k, "1" if k in env else "0")
     dv = to_dev(co)
-    need = ps.buffer_size(dims, 0, np.dtype(dtype).itemsize)
-    raw = torch.empty(need + 256, dtype=torch.uint8, device="cuda")
+    dirn = direction(len(dims), solvedim)
     with ps.Handle() as h:
-        ps.gpsv_batch(*(dv[k] for k in NAMES), 0, buffer=raw[16:16 + need], handle=h)
-        var = h.variant_that_ran(0)
-    assert ps.status_check()[1] == 0
-    assert "tma" not in var, var
-    assert fwd_err(dv["x"].cpu().numpy(), ref["x"]) <= tol, (dims, var)
+        if not buffer:
+            ps.gpsv_batch(*(dv[k] for k in NAMES), solvedim, buffer=None, handle=h)
+            assert ps.status_check()[1] == 0
+        elif offset is not None:
+            eb = dv["x"].element_size()
+            need = ps.buffer_size(list(dims), solvedim, eb)
+            raw = torch.empty(need + 256, dtype=torch.uint8, device="cuda")
+            solve_dev(dv, solvedim, handle=h, buffer=raw[offset:offset + need])
+        else:
+            solve_dev(dv, solvedim, handle=h)
+        var = h.variant_that_ran(dirn)
+    return dv["x"].cpu().numpy(), var
+
+
+CHAIN_DIMS = [(64, 64, 64), (48, 20, 33), (32, 40, 16), (20, 36, 9), (6, 40, 21),
+              (34, 17, 9), (40, 21, 5), (256, 3, 2), (200, 4, 3), (300, 4, 4), (18, 5, 4)]
+
+
+@pytest.mark.parametrize("dims", CHAIN_DIMS)
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_kernel_chain_every_direction(cuda, dims, dtype, monkeypatch):
+    """Each shape lands on the kernel its alignment and size allow -- the
+    Tensor-Memory kernel, the older TMA kernels (PENTA_NO_TMEM=1) or the
+    cp.async kernels (PENTA_NO_TMA=1) -- and every one agrees with the oracle.
+    Buffers aligned to 16 but not 128 bytes (no L2 discards) and to 8 bytes
+    only (no TMA), and no buffer at all, give the same answers."""
+    co = fixtures.random_dominant(dims, 56, dtype)
+    eb = np.dtype(dtype).itemsize
+    tol = FWD_TOL[dtype]
+    for solvedim in range(3):
+        if dims[solvedim] <= 4:
+            continue
+        ref = {k: co[k].astype(np.float64) for k in NAMES}
+        oracle.solve(ref["ds"], ref["dl"], ref["d"], ref["du"], ref["dw"], ref["x"], solvedim)
+        tm, old = _tmem_ok(dims, solvedim, eb), _old_tma_ok(dims, solvedim, eb)
+
+        def check(env, **kw):
+            got, var = _run_chain(co, solvedim, dims, env, monkeypatch, **kw)
+            assert fwd_err(got, ref["x"]) <= tol, (dims, solvedim, env, kw, var)
+            return var
+
+        v = check(())
+        assert ("tmem" in v) == tm and (tm or ("tma" in v) == old), (solvedim, v)
+        v = check(("PENTA_NO_TMEM",))
+        assert "tmem" not in v and ("tma" in v) == old, (solvedim, v)
+        v = check(("PENTA_NO_TMA",))
+        assert "tma" not in v and "tmem" not in v, (solvedim, v)
+        v = check((), offset=16)
+        assert ("tmem" in v) == tm, (solvedim, v)
+        # 8-byte aligned: no buffer-using TMA kernel (the strided one keeps its
+        # factors on chip and still runs)
+        v = check((), offset=8)
+        assert "tmem" not in v and ("tma" in v) == (old and solvedim != 0), (solvedim, v)
+        v = check((), buffer=False)
+        assert "tmem" not in v, (solvedim, v)
