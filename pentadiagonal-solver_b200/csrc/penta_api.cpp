@@ -449,8 +449,44 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
     case Algo::Transpose:  // x only: on-chip transpose, one thread per system
       if (run_tiled(1, "transpose")) return PENTAD_STATUS_SUCCESS;
       break;
+    case Algo::SharedFact: {  // line 0's coefficients for every line (not checked)
+      const size_t usable = buf ? std::min(buf_bytes, buffer_bytes(sh, sizeof(F))) : 0;
+      if (!env_flag("PENTA_NO_TMA") && sf_tmem_supported<F>(a, contig, ctx.smem_optin)) {
+        int occ;
+        const long long key = (1LL << 58) | ((long long)contig << 1) | (sizeof(F) == 8);
+        {
+          std::lock_guard<std::mutex> lock(ctx.mu);
+          auto it = ctx.occ_cache.find(key);
+          occ = (it != ctx.occ_cache.end()) ? it->second : -1;
+        }
+        if (occ < 0) {
+          occ = sf_tmem_occupancy<F>(contig);
+          std::lock_guard<std::mutex> lock(ctx.mu);
+          ctx.occ_cache[key] = occ;
+        }
+        if (occ == 1) {  // one CTA per SM: it owns all of Tensor Memory
+          err = launch_sf_tmem<F>(a, contig, ctx.sm_count, usable, stream);
+          if (err == cudaSuccess) {
+            record(ctx, dir, "shared-fact",
+                   contig ? "shared-fact:tmem S32 contig" : "shared-fact:tmem S32");
+            return PENTAD_STATUS_SUCCESS;
+          }
+          if (debug)
+            std::fprintf(stderr, "[penta] shared-fact tmem launch declined: %s\n",
+                         cudaGetErrorString(err));
+          cudaGetLastError();
+        }
+      }
+      if (usable < sf_lines_scratch_bytes<F>(sh.L)) {
+        *why = "shared-fact needs t_buffer of buffer_size_ext bytes for this shape";
+        return PENTAD_STATUS_INVALID_VALUE;
+      }
+      err = launch_sf_lines<F>(a, stream);
+      if (err != cudaSuccess) return PENTAD_STATUS_EXECUTION_FAILED;
+      record(ctx, dir, "shared-fact", "shared-fact:lines");
+      return PENTAD_STATUS_SUCCESS;
+    }
     case Algo::ThomasPcr:
-    case Algo::SharedFact:  // not built yet: the automatic choice serves it
     case Algo::Auto:
     default: {
       const int P = (lanes == 1) ? 1 : 2;

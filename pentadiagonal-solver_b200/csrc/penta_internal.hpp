@@ -93,6 +93,19 @@ template <typename F>
 cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count,
                         cudaStream_t stream);
 
+// shared_fact_kernels.cu: shared factorisation (line 0's coefficients for
+// every line).  The Tensor-Memory kernel needs no buffer (it caches its table
+// at the end of the buffer when there is one); the per-line fallback needs
+// sf_lines_scratch_bytes.
+template <typename F>
+bool sf_tmem_supported(const SolveArgs<F> &a, bool contig, int smem_optin);
+template <typename F> int sf_tmem_occupancy(bool contig);
+template <typename F>
+cudaError_t launch_sf_tmem(const SolveArgs<F> &a, bool contig, int sm_count,
+                           size_t usable_buf, cudaStream_t stream);
+template <typename F> size_t sf_lines_scratch_bytes(const Lines &L);
+template <typename F> cudaError_t launch_sf_lines(const SolveArgs<F> &a, cudaStream_t stream);
+
 // penta_status.cu: address of the device status word of `device` (the
 // current device when the address is first taken).
 int *device_status_word(int device);
