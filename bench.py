@@ -292,6 +292,49 @@ def run_ours(args):
             "algorithmic_bytes_per_launch": BYTES_PER_POINT_AXIS * n ** 3,
         },
     }
+    # ---- the same ADI run with shared factorisation (constant coefficients) --
+    # Algorithmic bytes: RHS read + solution written, 2 x 8 B per point per
+    # axis (the 5n-entry table is negligible).  Same field, same 50 x 3 solves.
+    sf_handle = ps.Handle()
+    for a in range(3):
+        sf_handle.set_algo(a, "shared-fact")
+    x.copy_(host["x"])
+
+    def sf_step():
+        for it in range(ITERS):
+            for axis in range(3):
+                ps.gpsv_batch(*(d[k] for k in names), x, axis, buffer=buf, stream=stream,
+                              handle=sf_handle)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            sf_step()
+    stream.synchronize()
+    if world > 1:
+        dist.barrier()
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    sf_steps = max(1, min(args.steps, 10))
+    with torch.cuda.stream(stream):
+        s0.record(stream)
+        for _ in range(sf_steps):
+            sf_step()
+        s1.record(stream)
+    stream.synchronize()
+    sf_ms = s0.elapsed_time(s1) / sf_steps
+    if world > 1:
+        t = torch.tensor([sf_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sf_ms = float(t.item())
+    sf_bytes = 2 * 8 * n ** 3 * 3 * ITERS
+    sf_gbs = world * sf_bytes / (sf_ms * 1e-3) / 1e9
+    result["shared_fact"] = {
+        "value": round(sf_gbs, 2), "unit": "GB/s", "ms_per_step": round(sf_ms, 4),
+        "bytes_per_point_axis": 16, "frac_of_peak": round(sf_gbs / world / peak, 4),
+        "kernel_variant": [sf_handle.variant_that_ran(a) for a in range(3)],
+        "systems_per_s": round(world * 3 * ITERS * n * n / (sf_ms * 1e-3), 1),
+    }
+    sf_handle.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(n, budget_s=args.cpu_seconds)
     handle.close()
