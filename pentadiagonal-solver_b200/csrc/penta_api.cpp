@@ -337,14 +337,15 @@ bool pick_tma_contig(Context &ctx, const SolveArgs<F> &a, size_t usable_buf,
 template <typename F>
 bool pick_tmem(Context &ctx, const SolveArgs<F> &a, bool contig, size_t usable_buf,
                TmemConfig &out) {
-  if (!tmem_supported<F>(a, contig, usable_buf)) return false;
+  bool w2s = false;
+  if (!tmem_supported<F>(a, contig, usable_buf, w2s)) return false;
   int want[2] = {-1, -1};
   if (const char *e = std::getenv("PENTA_TMEM_VARIANT"))
     std::sscanf(e, "%d,%d", &want[0], &want[1]);
   const std::vector<TmemConfig> &all = tmem_configs<F>();
   for (size_t i = 0; i < all.size(); ++i) {
     const TmemConfig &c = all[i];
-    if (c.contig != contig) continue;
+    if (c.contig != contig || c.w2s != w2s) continue;
     if ((want[0] >= 0 && c.stages != want[0]) || (want[1] >= 0 && c.xstages != want[1]))
       continue;
     if (c.smem > (size_t)ctx.smem_optin) continue;
@@ -497,8 +498,9 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
           err = launch_tmem<F>(a, mc, ctx.sm_count, stream);
           if (err == cudaSuccess) {
             char vb[96];
-            std::snprintf(vb, sizeof vb, "thomas-pcr:tmem P2 S16 R%d x%d/%d%s", mc.R,
-                          mc.stages, mc.xstages, contig ? " contig" : "");
+            std::snprintf(vb, sizeof vb, "thomas-pcr:tmem P2 S16 R%d x%d/%d%s%s", mc.R,
+                          mc.stages, mc.xstages, mc.w2s ? " w2s" : "",
+                          contig ? " contig" : "");
             record(ctx, dir, "thomas-pcr", vb);
             return PENTAD_STATUS_SUCCESS;
           }

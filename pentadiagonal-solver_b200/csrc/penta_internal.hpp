@@ -75,23 +75,39 @@ template <typename F> inline size_t tma_contig_scratch_bytes(const Lines &L) {
 }
 
 // tmem_kernels.cu: the Thomas kernel with its factors in Tensor Memory (all
-// directions; n <= 256 in FP64, n <= 512 in FP32; x2 goes through the
-// caller's buffer).
+// directions; n <= 512 in FP64, n <= 1024 in FP32; x2 -- and dw2 for the
+// longer lines -- go through the caller's buffer).  One grid per launch, or
+// many grids of one direction and precision in one batched launch.
 struct TmemConfig {
   bool contig;   // along x (rows contiguous) or strided
+  bool w2s;      // dw2 in the buffer (longer lines), du2 alone in TMEM
   int stages;    // forward ring stages per consumer warp
-  int xstages;   // x2 read-back stages per consumer warp
+  int xstages;   // read-back stages per consumer warp
   int R;         // rows per stage
   size_t smem;   // dynamic shared memory per CTA
 };
 template <typename F> const std::vector<TmemConfig> &tmem_configs();
 template <typename F> int tmem_occupancy(const TmemConfig &c);
-template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig);
+// A line set the kernel takes; `w2s` tells which factor mode it needs.
+template <typename F> bool tmem_shape(const Lines &L, bool contig, bool &w2s);
+template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig, bool w2s);
 template <typename F>
-bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf);
+bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf, bool &w2s);
 template <typename F>
 cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count,
                         cudaStream_t stream);
+// Batched: the job table (tmem_job_bytes() per grid) is filled on the host
+// and copied to device memory by the caller; grid i's scratch starts at
+// device_base + scratch_offsets[i] (128-byte aligned for L2 discards).
+template <typename F> size_t tmem_job_bytes();
+template <typename F>
+bool tmem_fill_jobs(const SolveArgs<F> *grids, int count, bool contig, bool w2s,
+                    unsigned char *device_base, void *host_jobs, size_t *scratch_offsets,
+                    int *total_tiles);
+template <typename F>
+cudaError_t launch_tmem_batch(const void *device_jobs, int n_jobs, int total_tiles, bool contig,
+                              bool w2s, bool discard, int sm_count, int *status,
+                              cudaStream_t stream);
 
 // shared_fact_kernels.cu: shared factorisation (line 0's coefficients for
 // every line).  The Tensor-Memory kernel needs no buffer (it caches its table

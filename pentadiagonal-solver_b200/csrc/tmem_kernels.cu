@@ -1,11 +1,12 @@
 // tmem_kernels.cu -- batched Thomas for all three directions with the
-// factors held in Tensor Memory.
+// factors held in Tensor Memory; one grid per launch, or many uneven grids in
+// one persistent launch.
 //
 // Algorithm (as tiled_kernels.cu with P = 2): a consumer warp owns tiles of 16
-// systems.  Lanes 0..15 eliminate the upper rows [0, m) of their system
-// downwards, lanes 16..31 the lower rows [m, n) upwards on the mirrored band
-// (dw, du, d, dl, ds), the halves meet in a 4x4 interface solve done with warp
-// shuffles, and each half substitutes back towards its own end.
+// lines.  Lanes 0..15 eliminate the upper rows [0, m) of their line downwards,
+// lanes 16..31 the lower rows [m, n) upwards on the mirrored band (dw, du, d,
+// dl, ds), the halves meet in a 4x4 interface solve done with warp shuffles,
+// and each half substitutes back towards its own end.
 //
 // m = R ceil(n / 2R) is a multiple of the rows per stage R, and the lower half
 // is extended by v = 2m - n virtual rows ahead of its first real row (rows
@@ -17,22 +18,30 @@
 //
 // Per CTA (one per SM): warps 0..3 compute, warps 4..7 feed them.
 //  * Producer warp 4 + c fills consumer c's ring of ST stages.  A stage is 12
-//    TMA tiles (6 arrays x 2 halves) of R rows x 16 systems on one mbarrier;
+//    TMA tiles (6 arrays x 2 halves) of R rows x 16 lines on one mbarrier;
 //    the lower half's tiles come from the mirrored arrays.  The consumer
 //    copies a stage into registers and releases the slot at once.
-//  * The factors du2, dw2 of every row go to Tensor Memory with one
-//    tcgen05.st of 32 columns per stage (consumer c uses TMEM lanes
-//    32c..32c+31, the lane quarter its warp can reach; FP64 rows take 4
-//    columns, FP32 rows 2).  512 columns hold m <= 16 R rows: n <= 256 in
-//    FP64, n <= 512 in FP32.  They come back with one tcgen05.ld per stage.
-//  * x2 makes an L2 round trip through the caller's buffer ([tile][half][m]
-//    [16]), written once per row and read back, most recent first, by two
-//    bulk copies per stage into a small ring; each 128-byte line is dropped
-//    from L2 (discard.global.L2) once read, so it never reaches HBM.
-//  * Output: strided directions store x directly (16 consecutive systems are
-//    one 128-byte segment).  Along x, a lane's rows are contiguous in memory:
-//    the R results per half go into a 64-byte-swizzled shared tile (the layout
-//    of the loads) and leave as TMA tile stores.
+//  * Factors in Tensor Memory (consumer c uses TMEM lanes 32c..32c+31, the
+//    lane quarter its warp can reach), one tcgen05.st per stage on the way
+//    down and one tcgen05.ld per stage on the way back:
+//      - du2 and dw2 (W2S = false): 4 columns per FP64 row, 2 per FP32 row;
+//        512 columns hold m <= 128 (FP64) / 256 (FP32) rows, n <= 256 / 512;
+//      - du2 only (W2S = true): half the columns, n <= 512 / 1024, with dw2
+//        travelling with x2 through the caller's buffer.
+//  * x2 (and dw2 when W2S) make an L2 round trip through the caller's buffer
+//    ([tile][half][m][16] of x2 or (dw2, x2) pairs), written once per row and
+//    read back, most recent first, by two bulk copies per stage into a small
+//    ring; each 128-byte line is dropped from L2 (discard.global.L2) once read,
+//    so it never reaches HBM.
+//  * Output: strided directions store x directly (16 consecutive lines are one
+//    128-byte segment).  Along x, a lane's rows are contiguous in memory: the R
+//    results per half go into a 64-byte-swizzled shared tile (the layout of the
+//    loads) and leave as TMA tile stores.
+//
+// Grids are described by jobs (tensor maps, x, buffer region, geometry).  A
+// single-grid launch passes its job as a kernel parameter; a batched launch
+// reads a job table from device memory and walks the concatenated tile list
+// of all its grids, so one launch -- and one CUDA-graph node -- solves them all.
 //
 // Tensor views: along x {n, n_sys} with tiles {R, 16} (64-byte rows, 64-byte
 // swizzle); strided {inner, n, outer} with tiles {16, R, 1}.  TMA needs
@@ -45,77 +54,83 @@
 // flight into its buffers (again bounded) and the CTA frees its TMEM before
 // returning.  A zero or non-finite pivot turns the carries into NaN or
 // infinity, which is checked once per tile (STATUS_ZERO_PIVOT_BIT).
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <type_traits>
+#include <vector>
 
 #include "penta_internal.hpp"
 #include "tma_device.cuh"
 
 namespace penta {
+
+// One grid of a launch.  Layout shared by host and device; 64-byte aligned
+// for the tensor maps.
+template <typename F> struct alignas(64) TmemJob {
+  CUtensorMap maps[6];  // ds, dl, d, du, dw, x
+  F *x;
+  F *scratch;           // this grid's region of the caller's buffer
+  int n, mt, inner, tpr, n_sys, n_tiles, tile_base, pad_;
+};
+
 namespace {
 
-constexpr int TS = 16;              // systems per tile
+constexpr int TS = 16;              // lines per tile
 constexpr int NCONS = 4;            // consumer warps per CTA, one per TMEM lane quarter
 constexpr uint32_t kTmemCols = 512; // the whole of Tensor Memory
-constexpr int kColsPerStage = 32;
 
 template <typename F, bool CONTIG> constexpr int tmem_rows_per_stage() {
   return CONTIG ? 64 / (int)sizeof(F) : 1024 / (TS * (int)sizeof(F));
 }
+// TMEM columns per stage: R rows of du2, dw2 (or du2 alone), sizeof(F)/4 each.
+template <typename F, bool W2S> constexpr int tmem_cols_per_stage() {
+  return 64 / (int)sizeof(F) * (W2S ? 1 : 2) * (int)sizeof(F) / 4;
+}
 
-template <typename F, bool CONTIG, int ST, int XST> struct TmemGeom {
+template <typename F, bool CONTIG, bool W2S, int ST, int XST> struct TmemGeom {
   static constexpr int R = tmem_rows_per_stage<F, CONTIG>();
-  static constexpr int BOX = R * TS;                 // elements per TMA tile
-  static constexpr int SE = 12 * BOX;                // forward stage
-  static constexpr int XE = 2 * R * TS;              // x2 read-back stage
-  static constexpr int OBE = CONTIG ? 4 * BOX : 0;   // output tiles: 2 buffers x 2 halves
+  static constexpr int PW = W2S ? 2 : 1;              // scratch values per row
+  static constexpr int BOX = R * TS;                  // elements per TMA tile
+  static constexpr int SE = 12 * BOX;                 // forward stage
+  static constexpr int XE = 2 * R * TS * PW;          // read-back stage
+  static constexpr int OBE = CONTIG ? 4 * BOX : 0;    // output tiles: 2 buffers x 2 halves
+  static constexpr int kCols = tmem_cols_per_stage<F, W2S>();
   static constexpr size_t kData = (size_t)(ST * SE + XST * XE + OBE) * sizeof(F);
   static constexpr size_t kBars = (size_t)(2 * ST + XST) * 8;
   static constexpr size_t kCons = (kData + kBars + 1023) / 1024 * 1024;
-  static constexpr size_t kTail = 64;                // TMEM address + stop flags
+  static constexpr size_t kTail = 64;                 // TMEM address + stop flags
   static constexpr size_t kUsed = NCONS * kCons + kTail + 1024;  // + alignment slack
   // at least 116 KB, so that one CTA holds an SM (and all of its TMEM)
   static constexpr size_t kSmem = kUsed > 118784 ? kUsed : 118784;
-  static_assert(R * (2 * (int)sizeof(F) / 4) == kColsPerStage, "32 TMEM columns per stage");
+  static_assert(R * (W2S ? 1 : 2) * (int)sizeof(F) / 4 == kCols, "TMEM columns per stage");
 };
 
-template <typename F> __device__ __forceinline__ void pack_factors(uint32_t (&tv)[32], int r,
-                                                                  F u, F w);
-template <> __device__ __forceinline__ void pack_factors<double>(uint32_t (&tv)[32], int r,
-                                                                 double u, double w) {
-  tv[4 * r + 0] = (uint32_t)__double2loint(u);
-  tv[4 * r + 1] = (uint32_t)__double2hiint(u);
-  tv[4 * r + 2] = (uint32_t)__double2loint(w);
-  tv[4 * r + 3] = (uint32_t)__double2hiint(w);
+template <typename F> __device__ __forceinline__ void put_bits(uint32_t *tv, int c, F v);
+template <> __device__ __forceinline__ void put_bits<double>(uint32_t *tv, int c, double v) {
+  tv[c] = (uint32_t)__double2loint(v);
+  tv[c + 1] = (uint32_t)__double2hiint(v);
 }
-template <> __device__ __forceinline__ void pack_factors<float>(uint32_t (&tv)[32], int r,
-                                                                float u, float w) {
-  tv[2 * r + 0] = __float_as_uint(u);
-  tv[2 * r + 1] = __float_as_uint(w);
+template <> __device__ __forceinline__ void put_bits<float>(uint32_t *tv, int c, float v) {
+  tv[c] = __float_as_uint(v);
 }
-template <typename F> __device__ __forceinline__ void unpack_factors(const uint32_t (&tv)[32],
-                                                                    int r, F &u, F &w);
-template <> __device__ __forceinline__ void unpack_factors<double>(const uint32_t (&tv)[32],
-                                                                   int r, double &u,
-                                                                   double &w) {
-  u = __hiloint2double((int)tv[4 * r + 1], (int)tv[4 * r + 0]);
-  w = __hiloint2double((int)tv[4 * r + 3], (int)tv[4 * r + 2]);
+template <typename F> __device__ __forceinline__ F get_bits(const uint32_t *tv, int c);
+template <> __device__ __forceinline__ double get_bits<double>(const uint32_t *tv, int c) {
+  return __hiloint2double((int)tv[c + 1], (int)tv[c]);
 }
-template <> __device__ __forceinline__ void unpack_factors<float>(const uint32_t (&tv)[32],
-                                                                  int r, float &u, float &w) {
-  u = __uint_as_float(tv[2 * r + 0]);
-  w = __uint_as_float(tv[2 * r + 1]);
+template <> __device__ __forceinline__ float get_bits<float>(const uint32_t *tv, int c) {
+  return __uint_as_float(tv[c]);
 }
 
-template <typename F, bool CONTIG, int ST, int XST>
+template <typename F, bool CONTIG, bool W2S, int ST, int XST, bool BATCH>
 __global__ void __launch_bounds__(64 * NCONS, 1)
-tmem_thomas_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
-                   F *__restrict__ scratch, int n, int mt, int inner, int tpr, int n_sys,
-                   int n_tiles, int flags, int *__restrict__ status_word) {
-  using G = TmemGeom<F, CONTIG, ST, XST>;
-  constexpr int R = G::R, BOX = G::BOX, SE = G::SE, XE = G::XE;
+tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__restrict__ jobs,
+                   int n_jobs, int total_tiles, int flags, int *__restrict__ status_word) {
+  using G = TmemGeom<F, CONTIG, W2S, ST, XST>;
+  using V2 = typename Vec2<F>::T;
+  constexpr int R = G::R, BOX = G::BOX, SE = G::SE, XE = G::XE, PW = G::PW;
   constexpr int EPC = 16 / (int)sizeof(F);  // elements per 16-byte chunk
+  constexpr int CW = (int)sizeof(F) / 4;    // TMEM columns per value
   constexpr int kMirror[6] = {4, 3, 2, 1, 0, 5};
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -127,7 +142,7 @@ tmem_thomas_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
   const int cons = warp % NCONS;  // the consumer this warp is, or feeds
   auto region = [&](int c) { return base + c * G::kCons; };
   F *const ring = reinterpret_cast<F *>(region(cons));
-  F *const xr = ring + ST * SE;    // x2 read-back stages [XST][2 halves][R][16]
+  F *const xr = ring + ST * SE;    // read-back stages [XST][2 halves][R][16][PW]
   F *const obuf = xr + XST * XE;   // along x: [2 buffers][2 halves][BOX]
   uint64_t *const full = reinterpret_cast<uint64_t *>(region(cons) + G::kData);
   uint64_t *const empty = full + ST;
@@ -135,11 +150,9 @@ tmem_thomas_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
   uint32_t *const tmem_slot = reinterpret_cast<uint32_t *>(base + NCONS * G::kCons);
   volatile int *const stop = reinterpret_cast<volatile int *>(tmem_slot + 4);  // [NCONS]
 
-  const int n_stages = mt / R;
-  const int nv = 2 * mt - n;  // virtual rows ahead of the lower half's first real row
   const int gw = blockIdx.x * NCONS + cons;
   const int tw = gridDim.x * NCONS;
-  const int my_tiles = gw < n_tiles ? (n_tiles - 1 - gw) / tw + 1 : 0;
+  const int my_tiles = gw < total_tiles ? (total_tiles - 1 - gw) / tw + 1 : 0;
 
   if (threadIdx.x == 0) {
     for (int c = 0; c < NCONS; ++c) {
@@ -155,23 +168,39 @@ tmem_thomas_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
   tmem_fence_after_sync();
   const uint32_t tmem_base = *tmem_slot;
 
-  auto tile_coords = [&](int tile, int &c0, int &c2) {
+  // the job of global tile t (t increases along a warp's sequence)
+  auto job_of = [&](int t, int &cursor) -> const TmemJob<F> * {
+    if constexpr (BATCH) {
+      while (cursor + 1 < n_jobs && jobs[cursor + 1].tile_base <= t) ++cursor;
+      return &jobs[cursor];
+    } else {
+      return &job1;
+    }
+  };
+  auto tile_coords = [&](const TmemJob<F> *J, int tile, int &c0, int &c2) {
     if (CONTIG) {
-      c0 = tile * TS;  // first system
+      c0 = tile * TS;  // first line
       c2 = 0;
     } else {
-      c2 = tile / tpr;  // run
-      c0 = (tile - c2 * tpr) * TS;
+      c2 = tile / J->tpr;  // run
+      c0 = (tile - c2 * J->tpr) * TS;
     }
   };
 
   // ================================ producer ================================
   if (warp >= NCONS) {
     if (lane != 0) return;
-    int slot = 0, use = 0;
+    int slot = 0, use = 0, cursor = 0, fenced = -1;
     for (int ti = 0; ti < my_tiles; ++ti) {
+      const int t = gw + ti * tw;
+      const TmemJob<F> *J = job_of(t, cursor);
+      if (BATCH && cursor != fenced) {  // host-written maps: acquire them once
+        for (int q = 0; q < 6; ++q) tensormap_acquire(&J->maps[q]);
+        fenced = cursor;
+      }
       int c0, c2;
-      tile_coords(gw + ti * tw, c0, c2);
+      tile_coords(J, t - J->tile_base, c0, c2);
+      const int n = J->n, mt = J->mt, n_stages = mt / R;
       for (int g = 0; g < n_stages; ++g) {
         if (use > 0 && !mbar_wait(&empty[slot], (unsigned)(use - 1) & 1u)) {
           atomicOr(status_word, STATUS_TIMEOUT_BIT);
@@ -186,14 +215,14 @@ tmem_thomas_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
           if (CONTIG) {
-            tma_load_2d(dst + (2 * q) * BOX, &maps.m[q], &full[slot], r_up, c0);
+            tma_load_2d(dst + (2 * q) * BOX, &J->maps[q], &full[slot], r_up, c0);
             if (lower)
-              tma_load_2d(dst + (2 * q + 1) * BOX, &maps.m[kMirror[q]], &full[slot], r_dn,
+              tma_load_2d(dst + (2 * q + 1) * BOX, &J->maps[kMirror[q]], &full[slot], r_dn,
                           c0);
           } else {
-            tma_load_3d(dst + (2 * q) * BOX, &maps.m[q], &full[slot], c0, r_up, c2);
+            tma_load_3d(dst + (2 * q) * BOX, &J->maps[q], &full[slot], c0, r_up, c2);
             if (lower)
-              tma_load_3d(dst + (2 * q + 1) * BOX, &maps.m[kMirror[q]], &full[slot], c0,
+              tma_load_3d(dst + (2 * q + 1) * BOX, &J->maps[kMirror[q]], &full[slot], c0,
                           r_dn, c2);
           }
         }
@@ -226,23 +255,26 @@ tmem_thomas_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
       st[r] = 0;
     }
   }
-  const int nvp = part ? nv : 0;  // this half's virtual rows
   const bool drop = (flags & 1) != 0;
 
-  int slot = 0, r_slot = 0, o_buf = 0;
+  int slot = 0, r_slot = 0, o_buf = 0, cursor = 0;
   unsigned phase = 0, r_phase = 0;
-  int consumed = 0;
   long long r_issued = 0, r_consumed = 0;
   bool bad = false, timed_out = false;
 
   for (int ti = 0; ti < my_tiles && !timed_out; ++ti) {
-    const int tile = gw + ti * tw;
+    const int t = gw + ti * tw;
+    const TmemJob<F> *J = job_of(t, cursor);
+    const int tile = t - J->tile_base;
     int c0, c2;
-    tile_coords(tile, c0, c2);
-    const int count = CONTIG ? min(TS, n_sys - c0) : min(TS, inner - c0);
+    tile_coords(J, tile, c0, c2);
+    const int n = J->n, mt = J->mt, inner = J->inner;
+    const int n_stages = mt / R;
+    const int nvp = part ? 2 * mt - n : 0;  // this half's virtual rows
+    const int count = CONTIG ? min(TS, J->n_sys - c0) : min(TS, inner - c0);
     const bool active = sys < count;
-    F *const x2t = scratch + (long long)tile * 2 * mt * TS;  // [2 halves][m][16]
-    F *const x2w = x2t + part * mt * TS + sys;               // row k at + k * 16
+    F *const x2t = J->scratch + (long long)tile * 2 * mt * TS * PW;  // [2][m][16][PW]
+    F *const x2w = x2t + (part * mt * TS + sys) * PW;                // row k at + k * 16 PW
 
     // ------------------------------ forward ---------------------------------
     Carry<F> c;
@@ -273,7 +305,6 @@ tmem_thomas_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
       fence_async_shared();
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[slot]);
-      ++consumed;
       if (++slot == ST) {
         slot = 0;
         phase ^= 1u;
@@ -283,13 +314,28 @@ tmem_thomas_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
       for (int r = 0; r < R; ++r)
         fwd_row_lean(a[r][0], a[r][1], a[r][2], a[r][3], a[r][4], a[r][5], c, u[r], w[r],
                      y[r]);
-      uint32_t tv[32];
+      uint32_t tv[G::kCols];
 #pragma unroll
-      for (int r = 0; r < R; ++r) pack_factors<F>(tv, r, u[r], w[r]);
-      tmem_store32(taddr + (uint32_t)(g * kColsPerStage), tv);
-      F *const x2g = x2w + g * R * TS;
+      for (int r = 0; r < R; ++r) {
+        put_bits<F>(tv, r * CW * (W2S ? 1 : 2), u[r]);
+        if (!W2S) put_bits<F>(tv, r * CW * 2 + CW, w[r]);
+      }
+      if constexpr (G::kCols == 32)
+        tmem_store32(taddr + (uint32_t)(g * G::kCols), reinterpret_cast<uint32_t(&)[32]>(tv));
+      else
+        tmem_store16(taddr + (uint32_t)(g * G::kCols), reinterpret_cast<uint32_t(&)[16]>(tv));
+      F *const x2g = x2w + g * R * TS * PW;
 #pragma unroll
-      for (int r = 0; r < R; ++r) x2g[r * TS] = y[r];
+      for (int r = 0; r < R; ++r) {
+        if constexpr (W2S) {
+          V2 pv;
+          pv.x = w[r];
+          pv.y = y[r];
+          *reinterpret_cast<V2 *>(x2g + r * TS * 2) = pv;
+        } else {
+          x2g[r * TS] = y[r];
+        }
+      }
     }
     if (timed_out) break;
     if (active)
@@ -318,15 +364,16 @@ tmem_thomas_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
 
     // ------------------------------ backward --------------------------------
     // stage s: elimination rows k in [m - (s+1) R, m - s R) of both halves
+    constexpr unsigned kBlock = (unsigned)(R * TS * PW * sizeof(F));  // one half, one stage
     int ri_slot = r_slot;
     auto rissue = [&](int s) {
       if (s >= n_stages) return;
       if (lane == 0) {
         const int k0 = mt - (s + 1) * R;
         F *dst = xr + ri_slot * XE;
-        mbar_expect_tx(&rfull[ri_slot], 2u * R * TS * (unsigned)sizeof(F));
-        bulk_load(dst, x2t + (long long)k0 * TS, R * TS * sizeof(F), &rfull[ri_slot]);
-        bulk_load(dst + R * TS, x2t + (long long)(mt + k0) * TS, R * TS * sizeof(F),
+        mbar_expect_tx(&rfull[ri_slot], 2u * kBlock);
+        bulk_load(dst, x2t + (long long)k0 * TS * PW, kBlock, &rfull[ri_slot]);
+        bulk_load(dst + R * TS * PW, x2t + (long long)(mt + k0) * TS * PW, kBlock,
                   &rfull[ri_slot]);
       }
       ++r_issued;
@@ -339,14 +386,29 @@ tmem_thomas_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
         timed_out = true;
         break;
       }
-      const F *xsrc = xr + r_slot * XE + part * R * TS + sys;
+      const F *xsrc = xr + r_slot * XE + (part * R * TS + sys) * PW;
       F xs[R], du[R], dw[R];
+      uint32_t tv[G::kCols];
+      if constexpr (G::kCols == 32)
+        tmem_load32(taddr + (uint32_t)((n_stages - 1 - s) * G::kCols),
+                    reinterpret_cast<uint32_t(&)[32]>(tv));
+      else
+        tmem_load16(taddr + (uint32_t)((n_stages - 1 - s) * G::kCols),
+                    reinterpret_cast<uint32_t(&)[16]>(tv));
 #pragma unroll
-      for (int r = 0; r < R; ++r) xs[r] = xsrc[(R - 1 - r) * TS];
-      uint32_t tv[32];
-      tmem_load32(taddr + (uint32_t)((n_stages - 1 - s) * kColsPerStage), tv);
-#pragma unroll
-      for (int r = 0; r < R; ++r) unpack_factors<F>(tv, R - 1 - r, du[r], dw[r]);
+      for (int r = 0; r < R; ++r) {
+        const int j = R - 1 - r;  // row inside the stage block
+        if constexpr (W2S) {
+          const V2 pv = *reinterpret_cast<const V2 *>(xsrc + j * TS * 2);
+          dw[r] = pv.x;
+          xs[r] = pv.y;
+          du[r] = get_bits<F>(tv, j * CW);
+        } else {
+          xs[r] = xsrc[j * TS];
+          du[r] = get_bits<F>(tv, j * CW * 2);
+          dw[r] = get_bits<F>(tv, j * CW * 2 + CW);
+        }
+      }
       if (CONTIG && lane == 0) bulk_wait_read<1>();  // output buffer o_buf is free
       fence_async_shared();
       __syncwarp();
@@ -356,9 +418,12 @@ tmem_thomas_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
         r_slot = 0;
         r_phase ^= 1u;
       }
-      if (drop && sys < 8)  // the stage's 1 KB of x2 per half is dead: drop it
-        discard_l2_line(x2t + (long long)(part * mt + mt - (s + 1) * R) * TS +
-                        sys * (128 / (int)sizeof(F)));
+      // the stage's block of each half is dead: drop its 128-byte lines
+      constexpr int kLines = (int)(kBlock / 128);
+      if (drop && sys < kLines)
+        discard_l2_line(reinterpret_cast<const unsigned char *>(
+                            x2t + (long long)(part * mt + mt - (s + 1) * R) * TS * PW) +
+                        sys * 128);
       F xk[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
@@ -373,8 +438,8 @@ tmem_thomas_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
         fence_async_shared();
         __syncwarp();
         if (lane == 0) {
-          tma_store_2d(&maps.m[5], ob, mt - (s + 1) * R, c0);
-          if (mt + s * R < n) tma_store_2d(&maps.m[5], ob + BOX, mt + s * R, c0);
+          tma_store_2d(&J->maps[5], ob, mt - (s + 1) * R, c0);
+          if (mt + s * R < n) tma_store_2d(&J->maps[5], ob + BOX, mt + s * R, c0);
           bulk_commit();
         }
         o_buf ^= 1;
@@ -382,7 +447,7 @@ tmem_thomas_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
         // the upper half runs towards row 0, the lower half towards row n - 1
         const int row0 = part ? (mt + s * R) : (mt - 1 - s * R);
         const long long step = part ? (long long)inner : -(long long)inner;
-        F *const p = x + (long long)c2 * inner * n + c0 + sys + (long long)row0 * inner;
+        F *const p = J->x + (long long)c2 * inner * n + c0 + sys + (long long)row0 * inner;
         if (part == 0 || mt + (s + 1) * R <= n) {
 #pragma unroll
           for (int r = 0; r < R; ++r) p[r * step] = xk[r];
@@ -414,7 +479,6 @@ tmem_thomas_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
     }
     if (lane == 0) atomicOr(status_word, STATUS_TIMEOUT_BIT);
   }
-  (void)consumed;
   if (CONTIG && lane == 0) bulk_wait<0>();
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status_word, STATUS_ZERO_PIVOT_BIT);
   // all consumers are done with Tensor Memory: warp 0 frees it
@@ -465,34 +529,71 @@ long long tile_count(const Lines &L, bool contig) {
   return contig ? (L.n_sys + TS - 1) / TS : (L.n_sys / L.inner) * ((L.inner + TS - 1) / TS);
 }
 
-template <typename F, bool CONTIG, int ST, int XST>
-cudaError_t tmem_launch(const SolveArgs<F> &a, int sm_count, cudaStream_t stream) {
-  using G = TmemGeom<F, CONTIG, ST, XST>;
-  TmaMaps maps;
+// Is this line set one the kernel takes (apart from the buffer)?  Also gives
+// whether it needs the dw2-in-buffer mode.
+template <typename F>
+bool shape_ok(const Lines &L, bool contig, bool &w2s) {
+  if (contig) {
+    if (L.inner != 1 || (L.n * sizeof(F)) % 16 != 0) return false;
+  } else {
+    if (L.inner <= 1 || (L.inner * sizeof(F)) % 16 != 0) return false;
+  }
+  const long long R =
+      contig ? tmem_rows_per_stage<F, true>() : tmem_rows_per_stage<F, false>();
+  const long long mt = split_row<F>(L, contig);
+  if (L.n - mt < 2) return false;  // two real rows per half
+  const long long stages = mt / R;
+  const long long cap_both = kTmemCols / tmem_cols_per_stage<F, false>();
+  const long long cap_du = kTmemCols / tmem_cols_per_stage<F, true>();
+  if (stages > cap_du) return false;
+  w2s = stages > cap_both;
+  if (L.n * L.n_sys >= (1LL << 31) || tile_count(L, contig) >= (1LL << 31)) return false;
+  return true;
+}
+
+template <typename F> size_t job_scratch_bytes(const Lines &L, bool contig, bool w2s) {
+  return (size_t)tile_count(L, contig) * 2 * (size_t)split_row<F>(L, contig) * TS *
+         (w2s ? 2 : 1) * sizeof(F);
+}
+
+template <typename F>
+bool fill_job(TmemJob<F> &J, const SolveArgs<F> &a, bool contig, F *scratch, int tile_base) {
+  std::memset(&J, 0, sizeof(J));
+  const int R = contig ? tmem_rows_per_stage<F, true>() : tmem_rows_per_stage<F, false>();
   const F *ptrs[6] = {a.ds, a.dl, a.d, a.du, a.dw, a.x};
   for (int q = 0; q < 6; ++q)
-    if (!encode<F>(&maps.m[q], ptrs[q], a.L, CONTIG, G::R)) return cudaErrorInvalidValue;
-  auto kern = tmem_thomas_kernel<F, CONTIG, ST, XST>;
+    if (!encode<F>(&J.maps[q], ptrs[q], a.L, contig, R)) return false;
+  J.x = a.x;
+  J.scratch = scratch;
+  J.n = (int)a.L.n;
+  J.mt = (int)split_row<F>(a.L, contig);
+  J.inner = (int)a.L.inner;
+  J.tpr = contig ? 1 : (int)((a.L.inner + TS - 1) / TS);
+  J.n_sys = (int)a.L.n_sys;
+  J.n_tiles = (int)tile_count(a.L, contig);
+  J.tile_base = tile_base;
+  return true;
+}
+
+template <typename F, bool CONTIG, bool W2S, int ST, int XST, bool BATCH>
+cudaError_t tmem_launch_raw(const TmemJob<F> &job1, const TmemJob<F> *jobs, int n_jobs,
+                            int total_tiles, int flags, int sm_count, int *status,
+                            cudaStream_t stream) {
+  using G = TmemGeom<F, CONTIG, W2S, ST, XST>;
+  auto kern = tmem_thomas_kernel<F, CONTIG, W2S, ST, XST, BATCH>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)G::kSmem);
   if (err != cudaSuccess) return err;
-  const int n = (int)a.L.n;
-  const int inner = (int)a.L.inner;
-  const int tpr = CONTIG ? 1 : (inner + TS - 1) / TS;
-  const long long n_tiles = tile_count(a.L, CONTIG);
-  const int mt = (int)split_row<F>(a.L, CONTIG);
-  const long long need = (n_tiles + NCONS - 1) / NCONS;
-  const int grid = (int)(need < sm_count ? need : sm_count);
-  const int flags = (reinterpret_cast<uintptr_t>(a.scratch) % 128 == 0) ? 1 : 0;  // L2 discards
-  kern<<<grid, 64 * NCONS, G::kSmem, stream>>>(maps, a.x, static_cast<F *>(a.scratch), n,
-                                                mt, inner, tpr, (int)a.L.n_sys,
-                                                (int)n_tiles, flags, a.status);
+  const int need = (total_tiles + NCONS - 1) / NCONS;
+  const int grid = need < sm_count ? need : sm_count;
+  if (grid <= 0) return cudaSuccess;
+  kern<<<grid, 64 * NCONS, G::kSmem, stream>>>(job1, jobs, n_jobs, total_tiles, flags, status);
   return cudaGetLastError();
 }
 
-template <typename F, bool CONTIG, int ST, int XST> int tmem_occ() {
-  using G = TmemGeom<F, CONTIG, ST, XST>;
-  auto kern = tmem_thomas_kernel<F, CONTIG, ST, XST>;
+template <typename F, bool CONTIG, bool W2S, int ST, int XST> int tmem_occ() {
+  using G = TmemGeom<F, CONTIG, W2S, ST, XST>;
+  auto kern = tmem_thomas_kernel<F, CONTIG, W2S, ST, XST, false>;
   int blocks = 0;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)G::kSmem) != cudaSuccess ||
@@ -506,24 +607,29 @@ template <typename F, bool CONTIG, int ST, int XST> int tmem_occ() {
 
 }  // namespace
 
-// (type, contiguous, forward stages, read-back stages); the first that fits
-// shared memory is the default.
-#define PENTA_TMEM_CONFIGS(X) \
-  X(double, true, 3, 4)       \
-  X(double, true, 3, 3)       \
-  X(double, false, 3, 4)      \
-  X(double, false, 4, 3)      \
-  X(float, true, 3, 4)        \
-  X(float, false, 3, 4)       \
-  X(float, false, 4, 3)
+// (type, contiguous, dw2 in the buffer, forward stages, read-back stages); for
+// each (type, layout, mode) the first variant is the default.  Batched
+// launches use the default variants.
+#define PENTA_TMEM_CONFIGS(X)   \
+  X(double, true, false, 3, 4)  \
+  X(double, true, false, 3, 3)  \
+  X(double, false, false, 3, 4) \
+  X(double, false, false, 4, 3) \
+  X(double, true, true, 3, 3)   \
+  X(double, false, true, 3, 4)  \
+  X(float, true, false, 3, 4)   \
+  X(float, false, false, 3, 4)  \
+  X(float, false, false, 4, 3)  \
+  X(float, true, true, 3, 3)    \
+  X(float, false, true, 3, 4)
 
 template <typename F> const std::vector<TmemConfig> &tmem_configs() {
   static const std::vector<TmemConfig> v = [] {
     std::vector<TmemConfig> out;
-#define PENTA_X(FT_, C_, ST_, XST_)                                                    \
-  if (std::is_same<F, FT_>::value)                                                     \
-    out.push_back(TmemConfig{C_, ST_, XST_, TmemGeom<FT_, C_, ST_, XST_>::R,           \
-                             TmemGeom<FT_, C_, ST_, XST_>::kSmem});
+#define PENTA_X(FT_, C_, W_, ST_, XST_)                                                  \
+  if (std::is_same<F, FT_>::value)                                                       \
+    out.push_back(TmemConfig{C_, W_, ST_, XST_, TmemGeom<FT_, C_, W_, ST_, XST_>::R,     \
+                             TmemGeom<FT_, C_, W_, ST_, XST_>::kSmem});
     PENTA_TMEM_CONFIGS(PENTA_X)
 #undef PENTA_X
     return out;
@@ -532,36 +638,28 @@ template <typename F> const std::vector<TmemConfig> &tmem_configs() {
 }
 
 template <typename F> int tmem_occupancy(const TmemConfig &c) {
-#define PENTA_X(FT_, C_, ST_, XST_)                                                    \
-  if (std::is_same<F, FT_>::value && c.contig == C_ && c.stages == ST_ &&              \
-      c.xstages == XST_)                                                               \
-    return tmem_occ<FT_, C_, ST_, XST_>();
+#define PENTA_X(FT_, C_, W_, ST_, XST_)                                                  \
+  if (std::is_same<F, FT_>::value && c.contig == C_ && c.w2s == W_ && c.stages == ST_ && \
+      c.xstages == XST_)                                                                 \
+    return tmem_occ<FT_, C_, W_, ST_, XST_>();
   PENTA_TMEM_CONFIGS(PENTA_X)
 #undef PENTA_X
   return 0;
 }
 
-template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig) {
-  return (size_t)tile_count(L, contig) * 2 * (size_t)split_row<F>(L, contig) * TS * sizeof(F);
+template <typename F> bool tmem_shape(const Lines &L, bool contig, bool &w2s) {
+  return tensor_map_encoder() != nullptr && shape_ok<F>(L, contig, w2s);
+}
+
+template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig, bool w2s) {
+  return job_scratch_bytes<F>(L, contig, w2s);
 }
 
 template <typename F>
-bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf) {
-  if (tensor_map_encoder() == nullptr) return false;
-  const Lines &L = a.L;
-  if (contig) {
-    if (L.inner != 1 || (L.n * sizeof(F)) % 16 != 0) return false;
-  } else {
-    if (L.inner <= 1 || (L.inner * sizeof(F)) % 16 != 0) return false;
-  }
-  const long long R =
-      contig ? tmem_rows_per_stage<F, true>() : tmem_rows_per_stage<F, false>();
-  const long long mt = split_row<F>(L, contig);
-  if (L.n - mt < 2) return false;                          // two real rows per half
-  if (mt / R > (long long)(kTmemCols / kColsPerStage)) return false;  // TMEM capacity
-  if (L.n * L.n_sys >= (1LL << 31) || tile_count(L, contig) >= (1LL << 31)) return false;
+bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf, bool &w2s) {
+  if (!tmem_shape<F>(a.L, contig, w2s)) return false;
   if (a.scratch == nullptr || reinterpret_cast<uintptr_t>(a.scratch) % 16 != 0 ||
-      tmem_scratch_bytes<F>(L, contig) > usable_buf)
+      tmem_scratch_bytes<F>(a.L, contig, w2s) > usable_buf)
     return false;
   const void *ptrs[6] = {a.ds, a.dl, a.d, a.du, a.dw, a.x};
   for (const void *p : ptrs)
@@ -572,27 +670,84 @@ bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf) {
 template <typename F>
 cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count,
                         cudaStream_t stream) {
-#define PENTA_X(FT_, C_, ST_, XST_)                                                    \
-  if (std::is_same<F, FT_>::value && c.contig == C_ && c.stages == ST_ &&              \
-      c.xstages == XST_)                                                               \
-    return tmem_launch<FT_, C_, ST_, XST_>(reinterpret_cast<const SolveArgs<FT_> &>(a), \
-                                           sm_count, stream);
+  TmemJob<F> J;
+  if (!fill_job<F>(J, a, c.contig, static_cast<F *>(a.scratch), 0))
+    return cudaErrorInvalidValue;
+  const int flags = (reinterpret_cast<uintptr_t>(a.scratch) % 128 == 0) ? 1 : 0;
+#define PENTA_X(FT_, C_, W_, ST_, XST_)                                                   \
+  if (std::is_same<F, FT_>::value && c.contig == C_ && c.w2s == W_ && c.stages == ST_ &&  \
+      c.xstages == XST_)                                                                  \
+    return tmem_launch_raw<FT_, C_, W_, ST_, XST_, false>(                                \
+        reinterpret_cast<const TmemJob<FT_> &>(J), nullptr, 1, J.n_tiles, flags, sm_count, \
+        a.status, stream);
   PENTA_TMEM_CONFIGS(PENTA_X)
 #undef PENTA_X
   return cudaErrorInvalidConfiguration;
+}
+
+// ---- batched launches -------------------------------------------------------
+template <typename F> size_t tmem_job_bytes() { return sizeof(TmemJob<F>); }
+
+template <typename F>
+bool tmem_fill_jobs(const SolveArgs<F> *grids, int count, bool contig, bool w2s,
+                    unsigned char *device_base, void *host_jobs, size_t *scratch_offsets,
+                    int *total_tiles) {
+  TmemJob<F> *J = static_cast<TmemJob<F> *>(host_jobs);
+  int tiles = 0;
+  for (int i = 0; i < count; ++i) {
+    F *scratch = reinterpret_cast<F *>(device_base + scratch_offsets[i]);
+    if (!fill_job<F>(J[i], grids[i], contig, scratch, tiles)) return false;
+    tiles += J[i].n_tiles;
+  }
+  *total_tiles = tiles;
+  (void)w2s;
+  return true;
+}
+
+template <typename F>
+cudaError_t launch_tmem_batch(const void *device_jobs, int n_jobs, int total_tiles, bool contig,
+                              bool w2s, bool discard, int sm_count, int *status,
+                              cudaStream_t stream) {
+  TmemJob<F> none;
+  std::memset(&none, 0, sizeof(none));
+  const TmemJob<F> *jobs = static_cast<const TmemJob<F> *>(device_jobs);
+  const int flags = discard ? 1 : 0;
+  if (contig && !w2s)
+    return tmem_launch_raw<F, true, false, 3, 4, true>(none, jobs, n_jobs, total_tiles, flags,
+                                                       sm_count, status, stream);
+  if (contig && w2s)
+    return tmem_launch_raw<F, true, true, 3, 3, true>(none, jobs, n_jobs, total_tiles, flags,
+                                                      sm_count, status, stream);
+  if (!w2s)
+    return tmem_launch_raw<F, false, false, 3, 4, true>(none, jobs, n_jobs, total_tiles, flags,
+                                                        sm_count, status, stream);
+  return tmem_launch_raw<F, false, true, 3, 4, true>(none, jobs, n_jobs, total_tiles, flags,
+                                                     sm_count, status, stream);
 }
 
 template const std::vector<TmemConfig> &tmem_configs<double>();
 template const std::vector<TmemConfig> &tmem_configs<float>();
 template int tmem_occupancy<double>(const TmemConfig &);
 template int tmem_occupancy<float>(const TmemConfig &);
-template size_t tmem_scratch_bytes<double>(const Lines &, bool);
-template size_t tmem_scratch_bytes<float>(const Lines &, bool);
-template bool tmem_supported<double>(const SolveArgs<double> &, bool, size_t);
-template bool tmem_supported<float>(const SolveArgs<float> &, bool, size_t);
+template bool tmem_shape<double>(const Lines &, bool, bool &);
+template bool tmem_shape<float>(const Lines &, bool, bool &);
+template size_t tmem_scratch_bytes<double>(const Lines &, bool, bool);
+template size_t tmem_scratch_bytes<float>(const Lines &, bool, bool);
+template bool tmem_supported<double>(const SolveArgs<double> &, bool, size_t, bool &);
+template bool tmem_supported<float>(const SolveArgs<float> &, bool, size_t, bool &);
 template cudaError_t launch_tmem<double>(const SolveArgs<double> &, const TmemConfig &, int,
                                          cudaStream_t);
 template cudaError_t launch_tmem<float>(const SolveArgs<float> &, const TmemConfig &, int,
                                         cudaStream_t);
+template size_t tmem_job_bytes<double>();
+template size_t tmem_job_bytes<float>();
+template bool tmem_fill_jobs<double>(const SolveArgs<double> *, int, bool, bool, unsigned char *,
+                                     void *, size_t *, int *);
+template bool tmem_fill_jobs<float>(const SolveArgs<float> *, int, bool, bool, unsigned char *,
+                                    void *, size_t *, int *);
+template cudaError_t launch_tmem_batch<double>(const void *, int, int, bool, bool, bool, int,
+                                               int *, cudaStream_t);
+template cudaError_t launch_tmem_batch<float>(const void *, int, int, bool, bool, bool, int,
+                                              int *, cudaStream_t);
 
 }  // namespace penta

@@ -259,9 +259,10 @@ def test_256cube_properties(cuda, solvedim):
 
 def _tmem_ok(dims, solvedim, eb):
     """Shapes the Tensor-Memory kernel takes: 16-byte aligned rows (x) or runs
-    (y, z), two real rows in each half of the split m = R ceil(n / 2R), at most
-    16 R rows per half (512 TMEM columns), and x2 scratch for whole tiles of 16
-    systems within the reference-sized buffer."""
+    (y, z), two real rows in each half of the split m = R ceil(n / 2R), m / R
+    stages within 512 TMEM columns (du2 and dw2 there: 16 stages; du2 alone,
+    dw2 in the buffer: 32 stages), and its scratch for whole tiles of 16 lines
+    within the reference-sized buffer."""
     n = dims[solvedim]
     inner = int(np.prod(dims[:solvedim]))
     n_sys = int(np.prod(dims)) // n
@@ -269,9 +270,13 @@ def _tmem_ok(dims, solvedim, eb):
     r = 64 // eb if contig else 1024 // (16 * eb)
     aligned = (n * eb) % 16 == 0 if contig else (inner > 1 and (inner * eb) % 16 == 0)
     mt = r * (-(-n // (2 * r)))
+    stages = mt // r
+    cols = r * eb // 4               # TMEM columns of one factor per stage
+    w2s = stages > 512 // (2 * cols)
     tiles = -(-n_sys // 16) if contig else (n_sys // inner) * -(-inner // 16)
+    need = tiles * 2 * mt * 16 * eb * (2 if w2s else 1)
     buf = ps.buffer_size(list(dims), solvedim, eb)
-    return aligned and n - mt >= 2 and mt // r <= 16 and tiles * 2 * mt * 16 * eb <= buf
+    return aligned and n - mt >= 2 and stages <= 512 // cols and need <= buf
 
 
 def _old_tma_ok(dims, solvedim, eb, buffer=True):
