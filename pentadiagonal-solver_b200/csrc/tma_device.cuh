@@ -62,6 +62,13 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
                : "memory");
 }
 
+// `count` arrivals at once.
+__device__ __forceinline__ void mbar_arrive_n(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(count)
+               : "memory");
+}
+
 // ---- proxy fences -----------------------------------------------------------
 // Orders this thread's generic shared-memory accesses before later async-proxy
 // (TMA / bulk copy) accesses of the same shared memory.
@@ -113,6 +120,20 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned b
       " [%0], [%1], %2, [%3];\n" ::"r"(smem_u32(dst)),
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
+}
+// Element copy global -> shared that writes zeros instead when !valid (the
+// source is then not read).
+template <int BYTES>
+__device__ __forceinline__ void cp_async_zfill(void *dst, const void *src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(smem_u32(dst)),
+               "l"(src), "n"(BYTES), "r"(valid ? BYTES : 0)
+               : "memory");
+}
+// Arrive on `bar` once all of this thread's earlier cp.async copies have landed
+// (counts as one of the barrier's expected arrivals).
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
 }
 __device__ __forceinline__ void bulk_commit() {
   asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");

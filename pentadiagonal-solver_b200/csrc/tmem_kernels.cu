@@ -68,10 +68,12 @@ namespace penta {
 // One grid of a launch.  Layout shared by host and device; 64-byte aligned
 // for the tensor maps.
 template <typename F> struct alignas(64) TmemJob {
-  CUtensorMap maps[6];  // ds, dl, d, du, dw, x
+  CUtensorMap maps[6];  // ds, dl, d, du, dw, x (when tma)
+  const F *arr[6];      // the same arrays
   F *x;
   F *scratch;           // this grid's region of the caller's buffer
-  int n, mt, inner, tpr, n_sys, n_tiles, tile_base, pad_;
+  int n, mt, inner, tpr, n_sys, n_tiles, tile_base;
+  int tma;              // 1: TMA tiles; 0: element copies (misaligned grid)
 };
 
 namespace {
@@ -157,7 +159,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   if (threadIdx.x == 0) {
     for (int c = 0; c < NCONS; ++c) {
       uint64_t *f = reinterpret_cast<uint64_t *>(region(c) + G::kData);
-      for (int s = 0; s < 2 * ST + XST; ++s) mbar_init(&f[s], 1);
+      for (int s = 0; s < 2 * ST + XST; ++s) mbar_init(&f[s], s < ST ? 32 : 1);
       stop[c] = 0;
     }
     mbar_init_fence();
@@ -188,43 +190,89 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   };
 
   // ================================ producer ================================
+  // The whole warp: lane 0 issues TMA tiles (arriving for all 32 lanes), or
+  // all lanes copy elements of a misaligned grid.  full[] counts 32 arrivals.
   if (warp >= NCONS) {
-    if (lane != 0) return;
     int slot = 0, use = 0, cursor = 0, fenced = -1;
     for (int ti = 0; ti < my_tiles; ++ti) {
       const int t = gw + ti * tw;
       const TmemJob<F> *J = job_of(t, cursor);
-      if (BATCH && cursor != fenced) {  // host-written maps: acquire them once
-        for (int q = 0; q < 6; ++q) tensormap_acquire(&J->maps[q]);
+      const bool tma = J->tma != 0;
+      if (BATCH && tma && cursor != fenced) {  // host-written maps: acquire them once
+        if (lane == 0)
+          for (int q = 0; q < 6; ++q) tensormap_acquire(&J->maps[q]);
         fenced = cursor;
       }
       int c0, c2;
       tile_coords(J, t - J->tile_base, c0, c2);
-      const int n = J->n, mt = J->mt, n_stages = mt / R;
+      const int n = J->n, mt = J->mt, n_stages = mt / R, inner = J->inner;
       for (int g = 0; g < n_stages; ++g) {
-        if (use > 0 && !mbar_wait(&empty[slot], (unsigned)(use - 1) & 1u)) {
-          atomicOr(status_word, STATUS_TIMEOUT_BIT);
+        // lane 0 waits for the slot (the others park in the shuffle, issuing
+        // nothing) and reads the stop flag for the warp
+        int go = 1;
+        if (lane == 0) {
+          go = (use == 0 || mbar_wait(&empty[slot], (unsigned)(use - 1) & 1u)) ? 1 : 0;
+          if (go && stop[cons] != 0) go = 2;
+        }
+        go = __shfl_sync(0xffffffffu, go, 0);
+        if (go != 1) {
+          if (go == 0 && lane == 0) atomicOr(status_word, STATUS_TIMEOUT_BIT);
           return;
         }
-        if (stop[cons]) return;
         const int r_up = g * R;
         const int r_dn = 2 * mt - (g + 1) * R;  // lower half, virtual rows included
-        const bool lower = r_dn < n;            // else all rows are virtual: not loaded
-        mbar_expect_tx(&full[slot], (lower ? 12u : 6u) * BOX * (unsigned)sizeof(F));
         F *dst = ring + slot * SE;
+        if (tma) {
+          if (lane == 0) {
+            const bool lower = r_dn < n;  // else all rows are virtual: not loaded
+            mbar_arrive_n(&full[slot], 31);  // for the lanes that copy nothing
+            mbar_expect_tx(&full[slot], (lower ? 12u : 6u) * BOX * (unsigned)sizeof(F));
 #pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          if (CONTIG) {
-            tma_load_2d(dst + (2 * q) * BOX, &J->maps[q], &full[slot], r_up, c0);
-            if (lower)
-              tma_load_2d(dst + (2 * q + 1) * BOX, &J->maps[kMirror[q]], &full[slot], r_dn,
-                          c0);
-          } else {
-            tma_load_3d(dst + (2 * q) * BOX, &J->maps[q], &full[slot], c0, r_up, c2);
-            if (lower)
-              tma_load_3d(dst + (2 * q + 1) * BOX, &J->maps[kMirror[q]], &full[slot], c0,
-                          r_dn, c2);
+            for (int q = 0; q < 6; ++q) {
+              if (CONTIG) {
+                tma_load_2d(dst + (2 * q) * BOX, &J->maps[q], &full[slot], r_up, c0);
+                if (lower)
+                  tma_load_2d(dst + (2 * q + 1) * BOX, &J->maps[kMirror[q]], &full[slot],
+                              r_dn, c0);
+              } else {
+                tma_load_3d(dst + (2 * q) * BOX, &J->maps[q], &full[slot], c0, r_up, c2);
+                if (lower)
+                  tma_load_3d(dst + (2 * q + 1) * BOX, &J->maps[kMirror[q]], &full[slot], c0,
+                              r_dn, c2);
+              }
+            }
           }
+        } else {
+          // the same tiles, element by element; rows past n and lines past the
+          // grid read as zeros
+          for (int e = lane; e < 12 * BOX; e += 32) {
+            const int bx = e / BOX, idx = e - bx * BOX;
+            const int q = bx >> 1, h = bx & 1;
+            int s, rr, doff;
+            if (CONTIG) {
+              s = idx / R;
+              rr = idx - s * R;
+              doff = s * R + ((rr / EPC) ^ ((s >> 1) & 3)) * EPC + rr % EPC;
+            } else {
+              rr = idx / TS;
+              s = idx - rr * TS;
+              doff = idx;
+            }
+            const int row = h ? (r_dn + rr) : (r_up + rr);
+            const int which = h ? (q == 5 ? 5 : 4 - q) : q;
+            const F *src = J->arr[which];
+            bool valid = row < n;
+            long long off;
+            if (CONTIG) {
+              valid = valid && c0 + s < J->n_sys;
+              off = (long long)(c0 + s) * n + row;
+            } else {
+              valid = valid && c0 + s < inner;
+              off = (long long)c2 * inner * n + (long long)row * inner + c0 + s;
+            }
+            cp_async_zfill<sizeof(F)>(dst + bx * BOX + doff, valid ? src + off : src, valid);
+          }
+          cp_async_mbar_arrive(&full[slot]);
         }
         if (++slot == ST) {
           slot = 0;
@@ -431,7 +479,17 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         xb = xa;
         xa = xk[r];
       }
-      if (CONTIG) {
+      if (CONTIG && !J->tma) {  // misaligned grid: each lane writes its own rows
+        if (active) {
+          F *const p = J->x + (long long)(c0 + sys) * n;
+          const int row0 = part ? (mt + s * R) : (mt - 1 - s * R);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int row = part ? row0 + r : row0 - r;
+            if (row < n) p[row] = xk[r];
+          }
+        }
+      } else if (CONTIG) {
         F *const ob = obuf + o_buf * 2 * BOX;
 #pragma unroll
         for (int r = 0; r < R; ++r) ob[st[r]] = xk[r];
@@ -533,11 +591,7 @@ long long tile_count(const Lines &L, bool contig) {
 // whether it needs the dw2-in-buffer mode.
 template <typename F>
 bool shape_ok(const Lines &L, bool contig, bool &w2s) {
-  if (contig) {
-    if (L.inner != 1 || (L.n * sizeof(F)) % 16 != 0) return false;
-  } else {
-    if (L.inner <= 1 || (L.inner * sizeof(F)) % 16 != 0) return false;
-  }
+  if (contig ? L.inner != 1 : L.inner <= 1) return false;
   const long long R =
       contig ? tmem_rows_per_stage<F, true>() : tmem_rows_per_stage<F, false>();
   const long long mt = split_row<F>(L, contig);
@@ -551,6 +605,16 @@ bool shape_ok(const Lines &L, bool contig, bool &w2s) {
   return true;
 }
 
+// TMA applies when the row stride and every array are 16-byte aligned.
+template <typename F> bool tma_ok(const SolveArgs<F> &a, bool contig) {
+  if (tensor_map_encoder() == nullptr) return false;
+  if (contig ? (a.L.n * sizeof(F)) % 16 != 0 : (a.L.inner * sizeof(F)) % 16 != 0) return false;
+  const void *ptrs[6] = {a.ds, a.dl, a.d, a.du, a.dw, a.x};
+  for (const void *p : ptrs)
+    if (reinterpret_cast<uintptr_t>(p) % 16 != 0) return false;
+  return true;
+}
+
 template <typename F> size_t job_scratch_bytes(const Lines &L, bool contig, bool w2s) {
   return (size_t)tile_count(L, contig) * 2 * (size_t)split_row<F>(L, contig) * TS *
          (w2s ? 2 : 1) * sizeof(F);
@@ -561,8 +625,11 @@ bool fill_job(TmemJob<F> &J, const SolveArgs<F> &a, bool contig, F *scratch, int
   std::memset(&J, 0, sizeof(J));
   const int R = contig ? tmem_rows_per_stage<F, true>() : tmem_rows_per_stage<F, false>();
   const F *ptrs[6] = {a.ds, a.dl, a.d, a.du, a.dw, a.x};
-  for (int q = 0; q < 6; ++q)
-    if (!encode<F>(&J.maps[q], ptrs[q], a.L, contig, R)) return false;
+  J.tma = tma_ok<F>(a, contig) ? 1 : 0;
+  for (int q = 0; q < 6; ++q) {
+    J.arr[q] = ptrs[q];
+    if (J.tma && !encode<F>(&J.maps[q], ptrs[q], a.L, contig, R)) J.tma = 0;
+  }
   J.x = a.x;
   J.scratch = scratch;
   J.n = (int)a.L.n;
@@ -648,7 +715,7 @@ template <typename F> int tmem_occupancy(const TmemConfig &c) {
 }
 
 template <typename F> bool tmem_shape(const Lines &L, bool contig, bool &w2s) {
-  return tensor_map_encoder() != nullptr && shape_ok<F>(L, contig, w2s);
+  return shape_ok<F>(L, contig, w2s);
 }
 
 template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig, bool w2s) {
@@ -662,8 +729,8 @@ bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf, bool 
       tmem_scratch_bytes<F>(a.L, contig, w2s) > usable_buf)
     return false;
   const void *ptrs[6] = {a.ds, a.dl, a.d, a.du, a.dw, a.x};
-  for (const void *p : ptrs)
-    if (reinterpret_cast<uintptr_t>(p) % 16 != 0) return false;
+  for (const void *p : ptrs)  // element alignment (TMA needs 16 bytes; see tma_ok)
+    if (reinterpret_cast<uintptr_t>(p) % sizeof(F) != 0) return false;
   return true;
 }
 

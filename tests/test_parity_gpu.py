@@ -258,8 +258,8 @@ def test_256cube_properties(cuda, solvedim):
 
 
 def _tmem_ok(dims, solvedim, eb):
-    """Shapes the Tensor-Memory kernel takes: 16-byte aligned rows (x) or runs
-    (y, z), two real rows in each half of the split m = R ceil(n / 2R), m / R
+    """Shapes the Tensor-Memory kernel takes (TMA tiles when rows (x) or runs
+    (y, z) are 16-byte aligned, element copies otherwise): two real rows in each half of the split m = R ceil(n / 2R), m / R
     stages within 512 TMEM columns (du2 and dw2 there: 16 stages; du2 alone,
     dw2 in the buffer: 32 stages), and its scratch for whole tiles of 16 lines
     within the reference-sized buffer."""
@@ -268,7 +268,7 @@ def _tmem_ok(dims, solvedim, eb):
     n_sys = int(np.prod(dims)) // n
     contig = solvedim == 0
     r = 64 // eb if contig else 1024 // (16 * eb)
-    aligned = (n * eb) % 16 == 0 if contig else (inner > 1 and (inner * eb) % 16 == 0)
+    aligned = True if contig else inner > 1   # misaligned grids use element copies
     mt = r * (-(-n // (2 * r)))
     stages = mt // r
     cols = r * eb // 4               # TMEM columns of one factor per stage
