@@ -61,6 +61,67 @@ EXTERN_C PENTAD_API const char *pentadsolver_variant_that_ran(pentadsolver_handl
 
 EXTERN_C PENTAD_API const char *pentadsolver_status_string(pentadStatus_t status);
 
+/* ---- Plans: many grids in one persistent launch ---------------------------
+ * No counterpart in the reference.  A plan solves a fixed set of grids (any
+ * mix of shapes, one precision, one solvedim) with one launch of the batched
+ * Tensor-Memory kernel; grids that kernel does not take (lines too short or
+ * too long) are solved one by one inside the same execute.  Creating a plan
+ * writes its job table into the caller's buffer (a synchronous copy);
+ * executing it launches kernels on `stream` only, so an execute can be
+ * captured into a CUDA graph and replayed.  The grids' arrays and the buffer
+ * must stay valid and unmoved for the plan's lifetime; their contents may
+ * change between executes (x is solved in place each time). */
+typedef struct pentadsolver_grid {
+  const void *ds, *dl, *d, *du, *dw; /* prod(dims) elements each, dims[0] contiguous */
+  void *x;                           /* right-hand side in, solution out */
+  int ndim;
+  int dims[PENTAD_MAXDIM];
+} pentadsolver_grid_t;
+typedef struct pentadsolver_plan_s *pentadsolver_plan_t;
+
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_buffer_size(
+    pentadsolver_handle_t handle, int elem_bytes, int count, const pentadsolver_grid_t *grids,
+    int solvedim, size_t *bytes);
+/* `ctas` = 0 uses every SM; fewer leaves SMs to concurrent work. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_create(
+    pentadsolver_handle_t handle, int elem_bytes, int count, const pentadsolver_grid_t *grids,
+    int solvedim, void *buffer, size_t buffer_bytes, int ctas, pentadsolver_plan_t *plan);
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_execute(pentadsolver_plan_t plan,
+                                                              void *stream);
+EXTERN_C PENTAD_API const char *pentadsolver_plan_describe(pentadsolver_plan_t plan);
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_destroy(pentadsolver_plan_t plan);
+
+/* ---- Mixed precision: FP32 sweeps, FP64 residual and correction -----------
+ * No counterpart in the reference.  Solves the FP64 system with FP32 sweeps
+ * (the library's FP32 kernels on FP32 copies of the coefficients) and `steps`
+ * rounds of iterative refinement: r = b - A x in FP64, an FP32 sweep of r,
+ * x += d in FP64.  With `reuse_fp32_coefficients` the copies already in the
+ * buffer (from an earlier call with the same coefficients) are used as they
+ * are.  The buffer's first 16 bytes receive (max|last correction|, max|x|)
+ * of the last step, an estimate of the remaining forward error
+ * (pentadsolver_refine_estimate reads them). */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_refine_buffer_size(
+    pentadsolver_handle_t handle, const int *t_dims, int t_ndim, int t_solvedim, size_t *bytes);
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_D_gpsv_batch_refine(
+    pentadsolver_handle_t handle, const double *ds, const double *dl, const double *d,
+    const double *du, const double *dw, double *x, const int *t_dims, int t_ndim,
+    int t_solvedim, int steps, int reuse_fp32_coefficients, void *t_buffer,
+    size_t t_buffer_bytes, void *stream);
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_refine_estimate(const void *t_buffer,
+                                                                 void *stream, double *out);
+/* The same for a set of FP64 grids as one plan (executed with
+ * pentadsolver_plan_execute): one batched FP32 launch per sweep plus one
+ * launch per FP64 step; pentadsolver_plan_estimates gives (max|d|, max|x|)
+ * per grid. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_refine_plan_buffer_size(
+    pentadsolver_handle_t handle, int count, const pentadsolver_grid_t *grids, int solvedim,
+    size_t *bytes);
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_refine_plan_create(
+    pentadsolver_handle_t handle, int count, const pentadsolver_grid_t *grids, int solvedim,
+    int steps, void *buffer, size_t buffer_bytes, int ctas, pentadsolver_plan_t *plan);
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_estimates(pentadsolver_plan_t plan,
+                                                               void *stream, double *out);
+
 /* No counterpart in the reference.  An FP64 solve that allocates nothing and
  * takes no scratch buffer, for callers that cannot call cudaMalloc around a
  * solve: applications whose device memory is all owned by their own pool,

@@ -10,6 +10,7 @@
 #include <cuda_runtime_api.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
@@ -18,6 +19,7 @@
 #include <string>
 #include <unordered_map>
 #include <unordered_set>
+#include <vector>
 
 #include "pentad_common.hpp"
 #include "pentadsolver.hpp"
@@ -591,6 +593,321 @@ pentadStatus_t solve_ex(pentadsolver_handle_t h, const F *ds, const F *dl,
   return st;
 }
 
+// ---------------------------------------------------------------------------
+// Plans: many grids solved along one solvedim in one persistent launch
+// ---------------------------------------------------------------------------
+size_t round256(size_t v) { return (v + 255) & ~size_t(255); }
+
+struct PlanSingle {  // a grid the batched kernel does not take: solved alone
+  pentadsolver_grid_t g;
+  size_t offset, bytes;
+};
+
+struct Plan {
+  Context *ctx = nullptr;
+  int elem = 8, solvedim = 0;
+  bool contig = false, w2s = false, discard = false;
+  unsigned char *buffer = nullptr;
+  int n_jobs = 0, total_tiles = 0, ctas = 0;
+  std::vector<PlanSingle> singles;
+  std::string desc;
+  // mixed-precision refinement over the same grids (refine plans only)
+  bool refine = false;
+  int steps = 0, chunks = 0;
+  RefineGrid *table = nullptr;   // device
+  double *est = nullptr;         // device [count][2]
+  int count = 0;
+  Plan *fp32 = nullptr;          // the FP32 plan over the cast copies
+  ~Plan() { delete fp32; }
+};
+
+// Buffer layout of a plan: [job table][scratch of each batched grid][buffer
+// of each grid solved alone], every region 256-byte aligned.  `order` gets
+// the batched grids, heaviest lines first (tiles are dealt round-robin to the
+// consumer warps, so this balances the tail).
+template <typename F>
+pentadStatus_t plan_layout(Context &ctx, int count, const pentadsolver_grid_t *grids,
+                           int solvedim, std::vector<int> &order, std::vector<size_t> &offs,
+                           std::vector<PlanSingle> &singles, bool &w2s, size_t &total,
+                           const char **why) {
+  if (count < 1 || grids == nullptr) {
+    *why = "no grids";
+    return PENTAD_STATUS_INVALID_VALUE;
+  }
+  const bool contig = solvedim == 0;
+  std::vector<Shape> shapes(count);
+  std::vector<char> ok(count, 0), need_w2s(count, 0);
+  for (int i = 0; i < count; ++i) {
+    const pentadsolver_grid_t &g = grids[i];
+    pentadStatus_t st = make_shape(g.dims, g.ndim, solvedim, shapes[i], why);
+    if (st != PENTAD_STATUS_SUCCESS) return st;
+    if (!g.ds || !g.dl || !g.d || !g.du || !g.dw || !g.x) {
+      *why = "an array pointer is null";
+      return PENTAD_STATUS_INVALID_VALUE;
+    }
+    bool w = false;
+    bool aligned = true;
+    const void *ptrs[6] = {g.ds, g.dl, g.d, g.du, g.dw, g.x};
+    for (const void *p : ptrs) aligned = aligned && reinterpret_cast<uintptr_t>(p) % sizeof(F) == 0;
+    ok[i] = aligned && !env_flag("PENTA_NO_TMA") && tmem_shape<F>(shapes[i].L, contig, w);
+    need_w2s[i] = w;
+  }
+  (void)ctx;
+  w2s = false;
+  order.clear();
+  for (int i = 0; i < count; ++i)
+    if (ok[i]) {
+      order.push_back(i);
+      w2s = w2s || need_w2s[i];
+    }
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return shapes[a].L.n > shapes[b].L.n; });
+  size_t off = round256(order.size() * tmem_job_bytes<F>());
+  offs.assign(count, 0);
+  for (int i : order) {
+    offs[i] = off;
+    off += round256(tmem_scratch_bytes<F>(shapes[i].L, contig, w2s));
+  }
+  singles.clear();
+  for (int i = 0; i < count; ++i)
+    if (!ok[i]) {
+      const size_t b = buffer_bytes(shapes[i], sizeof(F));
+      singles.push_back(PlanSingle{grids[i], off, b});
+      off += round256(b);
+    }
+  total = off;
+  return PENTAD_STATUS_SUCCESS;
+}
+
+template <typename F>
+pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *grids,
+                          int solvedim, void *buffer, size_t buffer_bytes_given, int ctas,
+                          Plan *&out, const char **why) {
+  if (!ctx.init()) {
+    *why = "no usable CUDA device";
+    return PENTAD_STATUS_NOT_INITIALIZED;
+  }
+  std::vector<int> order;
+  std::vector<size_t> offs;
+  std::vector<PlanSingle> singles;
+  bool w2s = false;
+  size_t total = 0;
+  pentadStatus_t st =
+      plan_layout<F>(ctx, count, grids, solvedim, order, offs, singles, w2s, total, why);
+  if (st != PENTAD_STATUS_SUCCESS) return st;
+  if (buffer == nullptr || buffer_bytes_given < total ||
+      reinterpret_cast<uintptr_t>(buffer) % 256 != 0) {
+    *why = "the plan needs a 256-byte aligned buffer of pentadsolver_plan_buffer_size bytes";
+    return PENTAD_STATUS_INVALID_VALUE;
+  }
+  unsigned char *base = static_cast<unsigned char *>(buffer);
+  const bool contig = solvedim == 0;
+  int total_tiles = 0;
+  if (!order.empty()) {
+    std::vector<SolveArgs<F>> args;
+    std::vector<size_t> job_offs;
+    for (int i : order) {
+      const pentadsolver_grid_t &g = grids[i];
+      Shape sh;
+      make_shape(g.dims, g.ndim, solvedim, sh, why);
+      args.push_back(SolveArgs<F>{static_cast<const F *>(g.ds), static_cast<const F *>(g.dl),
+                                  static_cast<const F *>(g.d), static_cast<const F *>(g.du),
+                                  static_cast<const F *>(g.dw), static_cast<F *>(g.x), sh.L,
+                                  base + offs[i], 0, nullptr});
+      job_offs.push_back(offs[i]);
+    }
+    const size_t jb = tmem_job_bytes<F>();
+    void *host = std::aligned_alloc(64, round256(order.size() * jb));
+    if (host == nullptr) {
+      *why = "host memory for the job table";
+      return PENTAD_STATUS_ALLOC_FAILED;
+    }
+    if (!tmem_fill_jobs<F>(args.data(), (int)args.size(), contig, w2s, base, host,
+                           job_offs.data(), &total_tiles)) {
+      std::free(host);
+      *why = "tensor map encoding failed";
+      return PENTAD_STATUS_INTERNAL_ERROR;
+    }
+    const cudaError_t e = cudaMemcpy(base, host, order.size() * jb, cudaMemcpyHostToDevice);
+    std::free(host);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      *why = "copying the job table to the buffer";
+      return PENTAD_STATUS_EXECUTION_FAILED;
+    }
+  }
+  Plan *p = new Plan();
+  p->ctx = &ctx;
+  p->elem = sizeof(F);
+  p->solvedim = solvedim;
+  p->contig = contig;
+  p->w2s = w2s;
+  p->discard = true;  // every region is 256-byte aligned
+  p->buffer = base;
+  p->n_jobs = (int)order.size();
+  p->total_tiles = total_tiles;
+  p->ctas = (ctas > 0 && ctas < ctx.sm_count) ? ctas : ctx.sm_count;
+  p->singles = singles;
+  char d[160];
+  std::snprintf(d, sizeof d, "tmem-batch %s grids=%d tiles=%d%s ctas=%d alone=%d",
+                sizeof(F) == 8 ? "f64" : "f32", p->n_jobs, total_tiles, w2s ? " w2s" : "",
+                p->ctas, (int)singles.size());
+  p->desc = d;
+  out = p;
+  return PENTAD_STATUS_SUCCESS;
+}
+
+template <typename F> pentadStatus_t plan_run(Plan &p, cudaStream_t stream) {
+  Context &ctx = *p.ctx;
+  int *status = device_status_word(ctx.device);
+  if (status == nullptr) return PENTAD_STATUS_INTERNAL_ERROR;
+  if (p.n_jobs > 0) {
+    const cudaError_t e = launch_tmem_batch<F>(p.buffer, p.n_jobs, p.total_tiles, p.contig,
+                                               p.w2s, p.discard, p.ctas, status, stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return PENTAD_STATUS_EXECUTION_FAILED;
+    }
+  }
+  for (const PlanSingle &s : p.singles) {
+    const char *why = "";
+    const pentadStatus_t st =
+        solve<F>(ctx, static_cast<const F *>(s.g.ds), static_cast<const F *>(s.g.dl),
+                 static_cast<const F *>(s.g.d), static_cast<const F *>(s.g.du),
+                 static_cast<const F *>(s.g.dw), static_cast<F *>(s.g.x), s.g.dims, s.g.ndim,
+                 p.solvedim, p.buffer + s.offset, s.bytes, stream, &why);
+    if (st != PENTAD_STATUS_SUCCESS) return st;
+  }
+  return PENTAD_STATUS_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Mixed precision: FP32 sweeps, FP64 residual and correction
+// ---------------------------------------------------------------------------
+struct RefineLayout {
+  size_t s_coef, r, b, solve, total;  // offsets (after a 256-byte estimate slot)
+};
+RefineLayout refine_layout(const Shape &sh) {
+  const size_t N = (size_t)sh.L.n * (size_t)sh.L.n_sys;
+  RefineLayout l;
+  l.s_coef = 256;
+  l.r = l.s_coef + round256(5 * N * sizeof(float));
+  l.b = l.r + round256(N * sizeof(float));
+  l.solve = l.b + round256(N * sizeof(double));
+  l.total = l.solve + round256(buffer_bytes(sh, sizeof(float)));
+  return l;
+}
+
+RefineGrid refine_grid(const Shape &sh, const double *ds, const double *dl, const double *d,
+                       const double *du, const double *dw, double *x, unsigned char *coef32,
+                       float *r, double *b, double *est) {
+  const size_t N = (size_t)sh.L.n * (size_t)sh.L.n_sys;
+  float *s = reinterpret_cast<float *>(coef32);
+  RefineGrid g;
+  std::memset(&g, 0, sizeof(g));
+  g.ds = ds; g.dl = dl; g.d = d; g.du = du; g.dw = dw;
+  g.x = x;
+  g.b = b;
+  g.s_ds = s; g.s_dl = s + N; g.s_d = s + 2 * N; g.s_du = s + 3 * N; g.s_dw = s + 4 * N;
+  g.r = r;
+  g.est = est;
+  g.n_points = (long long)N;
+  g.n = (int)sh.L.n;
+  g.inner = (int)sh.L.inner;
+  return g;
+}
+
+pentadStatus_t refine_solve(Context &ctx, const double *ds, const double *dl, const double *d,
+                            const double *du, const double *dw, double *x, const int *dims,
+                            int ndim, int solvedim, int steps, int reuse, void *buffer,
+                            size_t bytes, cudaStream_t stream, const char **why) {
+  Shape sh;
+  pentadStatus_t st = make_shape(dims, ndim, solvedim, sh, why);
+  if (st != PENTAD_STATUS_SUCCESS) return st;
+  if (!ds || !dl || !d || !du || !dw || !x) {
+    *why = "an array pointer is null";
+    return PENTAD_STATUS_INVALID_VALUE;
+  }
+  if (steps < 0 || steps > 8) {
+    *why = "refinement steps must be in [0, 8]";
+    return PENTAD_STATUS_INVALID_VALUE;
+  }
+  const RefineLayout l = refine_layout(sh);
+  if (buffer == nullptr || bytes < l.total || reinterpret_cast<uintptr_t>(buffer) % 256 != 0) {
+    *why = "refinement needs a 256-byte aligned buffer of pentadsolver_refine_buffer_size bytes";
+    return PENTAD_STATUS_INVALID_VALUE;
+  }
+  if (!ctx.init()) {
+    *why = "no usable CUDA device";
+    return PENTAD_STATUS_NOT_INITIALIZED;
+  }
+  unsigned char *base = static_cast<unsigned char *>(buffer);
+  const RefineGrid g = refine_grid(sh, ds, dl, d, du, dw, x, base + l.s_coef,
+                                   reinterpret_cast<float *>(base + l.r),
+                                   reinterpret_cast<double *>(base + l.b),
+                                   reinterpret_cast<double *>(base));
+  const int chunks = refine_chunks(g.n_points);
+  auto step = [&](RefineStep k) {
+    return launch_refine_step(k, g, nullptr, 1, chunks, stream) == cudaSuccess;
+  };
+  auto sweep = [&]() {
+    return solve<float>(ctx, g.s_ds, g.s_dl, g.s_d, g.s_du, g.s_dw, g.r, dims, ndim, solvedim,
+                        base + l.solve, l.total - l.solve, stream, why);
+  };
+  if (!step(reuse ? RefineStep::Prepare : RefineStep::PrepareCast)) goto failed;
+  if ((st = sweep()) != PENTAD_STATUS_SUCCESS) return st;
+  if (!step(RefineStep::Lift)) goto failed;
+  for (int k = 0; k < steps; ++k) {
+    if (!step(RefineStep::Residual)) goto failed;
+    if ((st = sweep()) != PENTAD_STATUS_SUCCESS) return st;
+    if (!step(RefineStep::Correct)) goto failed;
+  }
+  return PENTAD_STATUS_SUCCESS;
+failed:
+  cudaGetLastError();
+  *why = "a refinement kernel failed to launch";
+  return PENTAD_STATUS_EXECUTION_FAILED;
+}
+
+// Refine plans: [grid table][estimates][per grid: FP32 coefficients, r, b][FP32 plan]
+pentadStatus_t refine_plan_layout(int count, const pentadsolver_grid_t *grids, int solvedim,
+                                  std::vector<Shape> &shapes, std::vector<size_t> &goffs,
+                                  size_t &fp32_off, const char **why) {
+  if (count < 1 || grids == nullptr) {
+    *why = "no grids";
+    return PENTAD_STATUS_INVALID_VALUE;
+  }
+  shapes.resize(count);
+  goffs.resize(count);
+  size_t off = round256(count * sizeof(RefineGrid)) + round256(count * 2 * sizeof(double));
+  for (int i = 0; i < count; ++i) {
+    pentadStatus_t st = make_shape(grids[i].dims, grids[i].ndim, solvedim, shapes[i], why);
+    if (st != PENTAD_STATUS_SUCCESS) return st;
+    const size_t N = (size_t)shapes[i].L.n * (size_t)shapes[i].L.n_sys;
+    goffs[i] = off;
+    off += round256(5 * N * sizeof(float)) + round256(N * sizeof(float)) +
+           round256(N * sizeof(double));
+  }
+  fp32_off = off;
+  return PENTAD_STATUS_SUCCESS;
+}
+
+// The FP32 grids of a refine plan (the cast coefficients and r).
+void refine_fp32_grids(int count, const pentadsolver_grid_t *grids,
+                       const std::vector<Shape> &shapes, const std::vector<size_t> &goffs,
+                       unsigned char *base, std::vector<pentadsolver_grid_t> &out) {
+  out.resize(count);
+  for (int i = 0; i < count; ++i) {
+    const size_t N = (size_t)shapes[i].L.n * (size_t)shapes[i].L.n_sys;
+    float *s = reinterpret_cast<float *>(base + goffs[i]);
+    float *r = reinterpret_cast<float *>(base + goffs[i] + round256(5 * N * sizeof(float)));
+    out[i] = grids[i];
+    out[i].ds = s; out[i].dl = s + N; out[i].d = s + 2 * N; out[i].du = s + 3 * N;
+    out[i].dw = s + 4 * N;
+    out[i].x = r;
+  }
+}
+
 size_t size_query(const int *dims, int ndim, int solvedim, size_t elem) {
   Shape sh;
   const char *why = "";
@@ -832,4 +1149,236 @@ extern "C" const char *pentadsolver_status_string(pentadStatus_t s) {
     case PENTAD_STATUS_ZERO_PIVOT: return "zero pivot";
   }
   return "unknown status";
+}
+
+// ===========================================================================
+// Plans and mixed-precision refinement (pentadsolver_ext.h)
+// ===========================================================================
+struct pentadsolver_plan_s {
+  penta::Plan *p;
+};
+
+extern "C" pentadStatus_t pentadsolver_plan_buffer_size(pentadsolver_handle_t h, int elem_bytes,
+                                                        int count,
+                                                        const pentadsolver_grid_t *grids,
+                                                        int solvedim, size_t *bytes) {
+  if (bytes == nullptr || (elem_bytes != 4 && elem_bytes != 8)) return PENTAD_STATUS_INVALID_VALUE;
+  Context *ctx = penta::resolve(h);
+  std::vector<int> order;
+  std::vector<size_t> offs;
+  std::vector<penta::PlanSingle> singles;
+  bool w2s = false;
+  const char *why = "";
+  pentadStatus_t st =
+      elem_bytes == 8
+          ? penta::plan_layout<double>(*ctx, count, grids, solvedim, order, offs, singles, w2s,
+                                       *bytes, &why)
+          : penta::plan_layout<float>(*ctx, count, grids, solvedim, order, offs, singles, w2s,
+                                      *bytes, &why);
+  return st;
+}
+
+extern "C" pentadStatus_t pentadsolver_plan_create(pentadsolver_handle_t h, int elem_bytes,
+                                                   int count, const pentadsolver_grid_t *grids,
+                                                   int solvedim, void *buffer,
+                                                   size_t buffer_bytes, int ctas,
+                                                   pentadsolver_plan_t *plan) {
+  if (plan == nullptr || (elem_bytes != 4 && elem_bytes != 8)) return PENTAD_STATUS_INVALID_VALUE;
+  *plan = nullptr;
+  Context *ctx = penta::resolve(h);
+  penta::Plan *p = nullptr;
+  const char *why = "";
+  pentadStatus_t st =
+      elem_bytes == 8
+          ? penta::plan_build<double>(*ctx, count, grids, solvedim, buffer, buffer_bytes, ctas,
+                                      p, &why)
+          : penta::plan_build<float>(*ctx, count, grids, solvedim, buffer, buffer_bytes, ctas,
+                                     p, &why);
+  if (st != PENTAD_STATUS_SUCCESS) {
+    if (penta::env_flag("PENTA_DEBUG_LAUNCH")) std::fprintf(stderr, "[penta] plan: %s\n", why);
+    return st;
+  }
+  *plan = new pentadsolver_plan_s{p};
+  return PENTAD_STATUS_SUCCESS;
+}
+
+extern "C" pentadStatus_t pentadsolver_plan_execute(pentadsolver_plan_t plan, void *stream) {
+  if (plan == nullptr || plan->p == nullptr) return PENTAD_STATUS_INVALID_VALUE;
+  penta::Plan &p = *plan->p;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (!p.refine)
+    return p.elem == 8 ? penta::plan_run<double>(p, s) : penta::plan_run<float>(p, s);
+  // refinement: cast, FP32 sweep, lift, then (residual, sweep, correct) x steps
+  auto step = [&](penta::RefineStep k) {
+    penta::RefineGrid none;
+    std::memset(&none, 0, sizeof(none));
+    return penta::launch_refine_step(k, none, p.table, p.count, p.chunks, s) == cudaSuccess;
+  };
+  pentadStatus_t st;
+  if (!step(penta::RefineStep::PrepareCast)) return PENTAD_STATUS_EXECUTION_FAILED;
+  if ((st = penta::plan_run<float>(*p.fp32, s)) != PENTAD_STATUS_SUCCESS) return st;
+  if (!step(penta::RefineStep::Lift)) return PENTAD_STATUS_EXECUTION_FAILED;
+  for (int k = 0; k < p.steps; ++k) {
+    if (!step(penta::RefineStep::Residual)) return PENTAD_STATUS_EXECUTION_FAILED;
+    if ((st = penta::plan_run<float>(*p.fp32, s)) != PENTAD_STATUS_SUCCESS) return st;
+    if (!step(penta::RefineStep::Correct)) return PENTAD_STATUS_EXECUTION_FAILED;
+  }
+  return PENTAD_STATUS_SUCCESS;
+}
+
+extern "C" const char *pentadsolver_plan_describe(pentadsolver_plan_t plan) {
+  if (plan == nullptr || plan->p == nullptr) return penta::kNone;
+  return plan->p->desc.c_str();
+}
+
+extern "C" pentadStatus_t pentadsolver_plan_destroy(pentadsolver_plan_t plan) {
+  if (plan == nullptr) return PENTAD_STATUS_INVALID_VALUE;
+  delete plan->p;
+  delete plan;
+  return PENTAD_STATUS_SUCCESS;
+}
+
+extern "C" pentadStatus_t pentadsolver_refine_buffer_size(pentadsolver_handle_t, const int *dims,
+                                                          int ndim, int solvedim,
+                                                          size_t *bytes) {
+  if (bytes == nullptr) return PENTAD_STATUS_INVALID_VALUE;
+  penta::Shape sh;
+  const char *why = "";
+  pentadStatus_t st = penta::make_shape(dims, ndim, solvedim, sh, &why);
+  if (st != PENTAD_STATUS_SUCCESS) return st;
+  *bytes = penta::refine_layout(sh).total;
+  return PENTAD_STATUS_SUCCESS;
+}
+
+extern "C" pentadStatus_t pentadsolver_D_gpsv_batch_refine(
+    pentadsolver_handle_t h, const double *ds, const double *dl, const double *d,
+    const double *du, const double *dw, double *x, const int *dims, int ndim, int solvedim,
+    int steps, int reuse_fp32_coefficients, void *buffer, size_t buffer_bytes, void *stream) {
+  Context *ctx = penta::resolve(h);
+  const char *why = "";
+  pentadStatus_t st = penta::refine_solve(*ctx, ds, dl, d, du, dw, x, dims, ndim, solvedim,
+                                          steps, reuse_fp32_coefficients, buffer, buffer_bytes,
+                                          static_cast<cudaStream_t>(stream), &why);
+  if (st != PENTAD_STATUS_SUCCESS && penta::env_flag("PENTA_DEBUG_LAUNCH"))
+    std::fprintf(stderr, "[penta] refine: %s\n", why);
+  return st;
+}
+
+extern "C" pentadStatus_t pentadsolver_refine_estimate(const void *buffer, void *stream,
+                                                       double *out) {
+  if (buffer == nullptr || out == nullptr) return PENTAD_STATUS_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaMemcpyAsync(out, buffer, 2 * sizeof(double), cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    cudaGetLastError();
+    return PENTAD_STATUS_EXECUTION_FAILED;
+  }
+  return PENTAD_STATUS_SUCCESS;
+}
+
+extern "C" pentadStatus_t pentadsolver_refine_plan_buffer_size(pentadsolver_handle_t h,
+                                                               int count,
+                                                               const pentadsolver_grid_t *grids,
+                                                               int solvedim, size_t *bytes) {
+  if (bytes == nullptr) return PENTAD_STATUS_INVALID_VALUE;
+  std::vector<penta::Shape> shapes;
+  std::vector<size_t> goffs;
+  size_t fp32_off = 0;
+  const char *why = "";
+  pentadStatus_t st =
+      penta::refine_plan_layout(count, grids, solvedim, shapes, goffs, fp32_off, &why);
+  if (st != PENTAD_STATUS_SUCCESS) return st;
+  // the FP32 plan's own layout over the cast grids (pointers do not matter here)
+  std::vector<pentadsolver_grid_t> g32;
+  penta::refine_fp32_grids(count, grids, shapes, goffs,
+                           reinterpret_cast<unsigned char *>(uintptr_t(256)), g32);
+  size_t plan_bytes = 0;
+  st = pentadsolver_plan_buffer_size(h, 4, count, g32.data(), solvedim, &plan_bytes);
+  if (st != PENTAD_STATUS_SUCCESS) return st;
+  *bytes = fp32_off + plan_bytes;
+  return PENTAD_STATUS_SUCCESS;
+}
+
+extern "C" pentadStatus_t pentadsolver_refine_plan_create(pentadsolver_handle_t h, int count,
+                                                          const pentadsolver_grid_t *grids,
+                                                          int solvedim, int steps, void *buffer,
+                                                          size_t buffer_bytes, int ctas,
+                                                          pentadsolver_plan_t *plan) {
+  if (plan == nullptr || steps < 0 || steps > 8) return PENTAD_STATUS_INVALID_VALUE;
+  *plan = nullptr;
+  size_t need = 0;
+  pentadStatus_t st = pentadsolver_refine_plan_buffer_size(h, count, grids, solvedim, &need);
+  if (st != PENTAD_STATUS_SUCCESS) return st;
+  if (buffer == nullptr || buffer_bytes < need || reinterpret_cast<uintptr_t>(buffer) % 256 != 0)
+    return PENTAD_STATUS_INVALID_VALUE;
+  Context *ctx = penta::resolve(h);
+  if (!ctx->init()) return PENTAD_STATUS_NOT_INITIALIZED;
+  std::vector<penta::Shape> shapes;
+  std::vector<size_t> goffs;
+  size_t fp32_off = 0;
+  const char *why = "";
+  st = penta::refine_plan_layout(count, grids, solvedim, shapes, goffs, fp32_off, &why);
+  if (st != PENTAD_STATUS_SUCCESS) return st;
+  unsigned char *base = static_cast<unsigned char *>(buffer);
+  std::vector<pentadsolver_grid_t> g32;
+  penta::refine_fp32_grids(count, grids, shapes, goffs, base, g32);
+  penta::Plan *fp32 = nullptr;
+  st = penta::plan_build<float>(*ctx, count, g32.data(), solvedim, base + fp32_off,
+                                buffer_bytes - fp32_off, ctas, fp32, &why);
+  if (st != PENTAD_STATUS_SUCCESS) return st;
+  // the grid table of the FP64 steps
+  std::vector<penta::RefineGrid> table(count);
+  double *est = reinterpret_cast<double *>(base + penta::round256(count * sizeof(penta::RefineGrid)));
+  int chunks = 0;
+  for (int i = 0; i < count; ++i) {
+    const pentadsolver_grid_t &g = grids[i];
+    const size_t N = (size_t)shapes[i].L.n * (size_t)shapes[i].L.n_sys;
+    unsigned char *gb = base + goffs[i];
+    float *r = reinterpret_cast<float *>(gb + penta::round256(5 * N * sizeof(float)));
+    double *b = reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(r) +
+                                           penta::round256(N * sizeof(float)));
+    table[i] = penta::refine_grid(shapes[i], static_cast<const double *>(g.ds),
+                                  static_cast<const double *>(g.dl),
+                                  static_cast<const double *>(g.d),
+                                  static_cast<const double *>(g.du),
+                                  static_cast<const double *>(g.dw), static_cast<double *>(g.x),
+                                  gb, r, b, est + 2 * i);
+    table[i].chunk_base = chunks;
+    chunks += penta::refine_chunks(table[i].n_points);
+  }
+  if (cudaMemcpy(base, table.data(), count * sizeof(penta::RefineGrid), cudaMemcpyHostToDevice) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    delete fp32;
+    return PENTAD_STATUS_EXECUTION_FAILED;
+  }
+  penta::Plan *p = new penta::Plan();
+  p->ctx = ctx;
+  p->elem = 8;
+  p->solvedim = solvedim;
+  p->refine = true;
+  p->steps = steps;
+  p->chunks = chunks;
+  p->table = reinterpret_cast<penta::RefineGrid *>(base);
+  p->est = est;
+  p->count = count;
+  p->fp32 = fp32;
+  p->desc = "refine steps=" + std::to_string(steps) + " over " + fp32->desc;
+  *plan = new pentadsolver_plan_s{p};
+  return PENTAD_STATUS_SUCCESS;
+}
+
+extern "C" pentadStatus_t pentadsolver_plan_estimates(pentadsolver_plan_t plan, void *stream,
+                                                      double *out) {
+  if (plan == nullptr || plan->p == nullptr || !plan->p->refine || out == nullptr)
+    return PENTAD_STATUS_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaMemcpyAsync(out, plan->p->est, 2 * plan->p->count * sizeof(double),
+                      cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    cudaGetLastError();
+    return PENTAD_STATUS_EXECUTION_FAILED;
+  }
+  return PENTAD_STATUS_SUCCESS;
 }

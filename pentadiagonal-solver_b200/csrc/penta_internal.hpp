@@ -122,6 +122,25 @@ cudaError_t launch_sf_tmem(const SolveArgs<F> &a, bool contig, int sm_count,
 template <typename F> size_t sf_lines_scratch_bytes(const Lines &L);
 template <typename F> cudaError_t launch_sf_lines(const SolveArgs<F> &a, cudaStream_t stream);
 
+// refine_kernels.cu: FP64 residual and correction steps of mixed-precision
+// refinement over one grid (passed by value) or a device table of grids.
+struct RefineGrid {
+  const double *ds, *dl, *d, *du, *dw;  // the FP64 problem
+  double *x;                            // the iterate (the caller's x)
+  double *b;                            // the saved right-hand side
+  float *s_ds, *s_dl, *s_d, *s_du, *s_dw;  // FP32 coefficient copies
+  float *r;                             // FP32 right-hand side / correction
+  double *est;                          // [max|last correction|, max|x|]
+  long long n_points;
+  int n, inner;                         // line length, row stride
+  int chunk_base;                       // first CTA of this grid in a table launch
+  int pad_;
+};
+enum class RefineStep { PrepareCast, Prepare, Lift, Residual, Correct };
+int refine_chunks(long long n_points);
+cudaError_t launch_refine_step(RefineStep step, const RefineGrid &one, const RefineGrid *table,
+                               int count, int total_chunks, cudaStream_t stream);
+
 // penta_status.cu: address of the device status word of `device` (the
 // current device when the address is first taken).
 int *device_status_word(int device);

@@ -1,0 +1,164 @@
+// refine_kernels.cu -- the FP64 steps of mixed-precision iterative refinement.
+//
+// A pentadiagonal system with FP64 coefficients A and right-hand side b is
+// solved with FP32 sweeps and refined:
+//     r0 = fl32(b);  x = solve32(A32, r0)            (FP32 sweep)
+//     repeat: r = fl32(b - A x)                       (FP64 residual)
+//             d = solve32(A32, r)                     (FP32 sweep)
+//             x = x + d                               (FP64 correction)
+// The residual and the correction are the only FP64 arithmetic; the sweeps
+// are the library's FP32 kernels.  Each kernel here walks the points of one
+// or many grids (a grid table; one CTA handles a chunk of one grid), so a
+// batch of uneven grids is one launch per step.
+//
+// The residual uses the same masking as the solvers: the couplings that leave
+// a line (ds at rows 0,1; dl at row 0; du at row n-1; dw at rows n-2,n-1) are
+// ignored whatever they hold.
+//
+// The correction step also records, per grid, max|d| and max|x| (non-negative
+// doubles compared as integers with atomicMax), whose ratio estimates the
+// forward error of the iterate before the step.
+#include <cstdint>
+
+#include "penta_internal.hpp"
+
+namespace penta {
+namespace {
+
+constexpr int kChunk = 4096;   // points per CTA
+constexpr int kThreads = 256;
+
+// The grid CTA `block` works on: `one` when there is no table.
+__device__ __forceinline__ const RefineGrid &grid_of(const RefineGrid &one,
+                                                     const RefineGrid *table, int count,
+                                                     int block, long long &first) {
+  if (table == nullptr) {
+    first = (long long)block * kChunk;
+    return one;
+  }
+  int lo = 0, hi = count - 1;  // last grid whose chunk_base <= block
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (table[mid].chunk_base <= block) lo = mid; else hi = mid - 1;
+  }
+  first = (long long)(block - table[lo].chunk_base) * kChunk;
+  return table[lo];
+}
+
+__global__ void __launch_bounds__(kThreads)
+rf_prepare_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__restrict__ table, int count, int cast_coefficients) {
+  long long first;
+  const RefineGrid &g = grid_of(one, table, count, blockIdx.x, first);
+  const long long end = min(first + kChunk, g.n_points);
+  for (long long i = first + threadIdx.x; i < end; i += kThreads) {
+    if (cast_coefficients) {
+      g.s_ds[i] = (float)g.ds[i];
+      g.s_dl[i] = (float)g.dl[i];
+      g.s_d[i] = (float)g.d[i];
+      g.s_du[i] = (float)g.du[i];
+      g.s_dw[i] = (float)g.dw[i];
+    }
+    const double b = g.x[i];
+    g.b[i] = b;
+    g.r[i] = (float)b;
+  }
+}
+
+// x = fl64(r) after the first FP32 sweep.
+__global__ void __launch_bounds__(kThreads)
+rf_lift_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__restrict__ table, int count) {
+  long long first;
+  const RefineGrid &g = grid_of(one, table, count, blockIdx.x, first);
+  const long long end = min(first + kChunk, g.n_points);
+  for (long long i = first + threadIdx.x; i < end; i += kThreads) g.x[i] = (double)g.r[i];
+}
+
+// r = fl32(b - A x), FP64 arithmetic.
+__global__ void __launch_bounds__(kThreads)
+rf_residual_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__restrict__ table, int count) {
+  long long first;
+  const RefineGrid &g = grid_of(one, table, count, blockIdx.x, first);
+  const long long end = min(first + kChunk, g.n_points);
+  const long long s = g.inner;
+  const int n = g.n;
+  for (long long i = first + threadIdx.x; i < end; i += kThreads) {
+    const int k = (int)((i / s) % n);  // row within its line
+    double ax = g.d[i] * g.x[i];
+    if (k >= 2) ax = fma(g.ds[i], g.x[i - 2 * s], ax);
+    if (k >= 1) ax = fma(g.dl[i], g.x[i - s], ax);
+    if (k <= n - 2) ax = fma(g.du[i], g.x[i + s], ax);
+    if (k <= n - 3) ax = fma(g.dw[i], g.x[i + 2 * s], ax);
+    g.r[i] = (float)(g.b[i] - ax);
+  }
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
+  // non-negative doubles order like their bit patterns
+  atomicMax(reinterpret_cast<unsigned long long *>(addr),
+            (unsigned long long)__double_as_longlong(v));
+}
+
+// x += fl64(d); est = (max|d|, max|x|) over the grid.
+__global__ void __launch_bounds__(kThreads)
+rf_correct_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__restrict__ table, int count) {
+  long long first;
+  const RefineGrid &g = grid_of(one, table, count, blockIdx.x, first);
+  const long long end = min(first + kChunk, g.n_points);
+  double md = 0.0, mx = 0.0;
+  for (long long i = first + threadIdx.x; i < end; i += kThreads) {
+    const double dd = (double)g.r[i];
+    const double xn = g.x[i] + dd;
+    g.x[i] = xn;
+    md = fmax(md, fabs(dd));
+    mx = fmax(mx, fabs(xn));
+  }
+  for (int o = 16; o > 0; o /= 2) {
+    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_nonneg(&g.est[0], md);
+    atomic_max_nonneg(&g.est[1], mx);
+  }
+}
+
+// Clear the estimate before a correction step.
+__global__ void rf_clear_kernel(const __grid_constant__ RefineGrid one,
+                                const RefineGrid *__restrict__ table, int count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) {
+    double *est = table ? table[i].est : one.est;
+    est[0] = 0.0;
+    est[1] = 0.0;
+  }
+}
+
+}  // namespace
+
+int refine_chunks(long long n_points) { return (int)((n_points + kChunk - 1) / kChunk); }
+
+cudaError_t launch_refine_step(RefineStep step, const RefineGrid &one, const RefineGrid *table,
+                               int count, int total_chunks, cudaStream_t stream) {
+  if (total_chunks <= 0) return cudaSuccess;
+  switch (step) {
+    case RefineStep::PrepareCast:
+      rf_prepare_kernel<<<total_chunks, kThreads, 0, stream>>>(one, table, count, 1);
+      break;
+    case RefineStep::Prepare:
+      rf_prepare_kernel<<<total_chunks, kThreads, 0, stream>>>(one, table, count, 0);
+      break;
+    case RefineStep::Lift:
+      rf_lift_kernel<<<total_chunks, kThreads, 0, stream>>>(one, table, count);
+      break;
+    case RefineStep::Residual:
+      rf_residual_kernel<<<total_chunks, kThreads, 0, stream>>>(one, table, count);
+      break;
+    case RefineStep::Correct:
+      rf_clear_kernel<<<(count + 127) / 128, 128, 0, stream>>>(one, table, count);
+      rf_correct_kernel<<<total_chunks, kThreads, 0, stream>>>(one, table, count);
+      break;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace penta

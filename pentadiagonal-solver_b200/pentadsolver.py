@@ -241,3 +241,176 @@ def alloc_buffer(dims, solvedim: int, dtype, device="cuda"):
 
 def library_loaded_path() -> str:
     return os.fspath(LIB_PATH)
+
+
+# ---------------------------------------------------------------------------
+# Plans (many grids, one persistent launch) and mixed-precision refinement
+# ---------------------------------------------------------------------------
+MAXDIM = 8
+
+
+class GridDesc(ctypes.Structure):
+    """pentadsolver_grid_t"""
+    _fields_ = [("ds", _P), ("dl", _P), ("d", _P), ("du", _P), ("dw", _P), ("x", _P),
+                ("ndim", _I), ("dims", _I * MAXDIM)]
+
+
+def _grid_descs(grids):
+    """grids: sequence of dicts with the six tensors ds, dl, d, du, dw, x."""
+    arr = (GridDesc * len(grids))()
+    for i, g in enumerate(grids):
+        _check_arrays([g[k] for k in ("ds", "dl", "d", "du", "dw", "x")])
+        dims = dims_of(g["x"])
+        arr[i].ds, arr[i].dl, arr[i].d = _ptr(g["ds"]), _ptr(g["dl"]), _ptr(g["d"])
+        arr[i].du, arr[i].dw, arr[i].x = _ptr(g["du"]), _ptr(g["dw"]), _ptr(g["x"])
+        arr[i].ndim = len(dims)
+        for k, v in enumerate(dims):
+            arr[i].dims[k] = v
+    return arr
+
+
+def _typed(name, argtypes, restype=_I):
+    f = getattr(lib(), name)
+    f.argtypes = argtypes
+    f.restype = restype
+    return f
+
+
+def _stream_ptr(stream, device):
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream(device)
+    return stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+
+
+class Plan:
+    """A fixed set of grids solved along ``solvedim`` by one persistent launch
+    (``pentadsolver_plan_create`` / ``_execute``).  ``refine_steps`` (FP64
+    grids only) makes it a mixed-precision plan: FP32 sweeps plus that many
+    FP64 residual/correction rounds.  The plan keeps references to the grids'
+    tensors and owns its buffer; execute() is capturable in a CUDA graph."""
+
+    def __init__(self, grids, solvedim: int, refine_steps: int | None = None, ctas: int = 0,
+                 handle=None):
+        import torch
+
+        self.grids = list(grids)
+        self.solvedim = int(solvedim)
+        self.refine = refine_steps is not None
+        self._descs = _grid_descs(self.grids)
+        x0 = self.grids[0]["x"]
+        self.device = x0.device
+        eb = x0.element_size()
+        n = len(self.grids)
+        size = ctypes.c_size_t(0)
+        if self.refine:
+            if x0.dtype != torch.float64:
+                raise ValueError("refinement plans take FP64 grids")
+            st = _typed("pentadsolver_refine_plan_buffer_size",
+                        [_P, _I, ctypes.POINTER(GridDesc), _I, ctypes.POINTER(_Z)])(
+                _hval(handle), n, self._descs, self.solvedim, ctypes.byref(size))
+        else:
+            st = _typed("pentadsolver_plan_buffer_size",
+                        [_P, _I, _I, ctypes.POINTER(GridDesc), _I, ctypes.POINTER(_Z)])(
+                _hval(handle), eb, n, self._descs, self.solvedim, ctypes.byref(size))
+        if st != SUCCESS:
+            raise PentadError(st, "plan buffer size")
+        self.buffer_bytes = max(int(size.value), 256)
+        self.buffer = torch.empty(self.buffer_bytes + 256, dtype=torch.uint8, device=self.device)
+        off = (-self.buffer.data_ptr()) % 256
+        self._buf = self.buffer[off:off + self.buffer_bytes]
+        self._plan = _P(None)
+        if self.refine:
+            st = _typed("pentadsolver_refine_plan_create",
+                        [_P, _I, ctypes.POINTER(GridDesc), _I, _I, _P, _Z, _I, ctypes.POINTER(_P)])(
+                _hval(handle), n, self._descs, self.solvedim, int(refine_steps), _ptr(self._buf),
+                self.buffer_bytes, int(ctas), ctypes.byref(self._plan))
+        else:
+            st = _typed("pentadsolver_plan_create",
+                        [_P, _I, _I, ctypes.POINTER(GridDesc), _I, _P, _Z, _I, ctypes.POINTER(_P)])(
+                _hval(handle), eb, n, self._descs, self.solvedim, _ptr(self._buf),
+                self.buffer_bytes, int(ctas), ctypes.byref(self._plan))
+        if st != SUCCESS:
+            raise PentadError(st, "plan create")
+
+    def execute(self, stream=None) -> None:
+        st = _typed("pentadsolver_plan_execute", [_P, _P])(
+            self._plan, _stream_ptr(stream, self.device))
+        if st != SUCCESS:
+            raise PentadError(st, "plan execute")
+
+    def describe(self) -> str:
+        return _typed("pentadsolver_plan_describe", [_P], ctypes.c_char_p)(self._plan).decode()
+
+    def estimates(self, stream=None):
+        """(max|last correction|, max|x|) per grid of a refinement plan."""
+        out = (ctypes.c_double * (2 * len(self.grids)))()
+        st = _typed("pentadsolver_plan_estimates", [_P, _P, _P])(
+            self._plan, _stream_ptr(stream, self.device), out)
+        if st != SUCCESS:
+            raise PentadError(st, "plan estimates")
+        return [(out[2 * i], out[2 * i + 1]) for i in range(len(self.grids))]
+
+    def close(self) -> None:
+        if getattr(self, "_plan", None) and self._plan.value:
+            _typed("pentadsolver_plan_destroy", [_P])(self._plan)
+            self._plan = _P(None)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def refine_buffer_size(dims, solvedim: int, handle=None) -> int:
+    size = ctypes.c_size_t(0)
+    st = _typed("pentadsolver_refine_buffer_size", [_P, _P, _I, _I, ctypes.POINTER(_Z)])(
+        _hval(handle), _dims(dims), len(dims), int(solvedim), ctypes.byref(size))
+    if st != SUCCESS:
+        raise PentadError(st, "refine buffer size")
+    return int(size.value)
+
+
+def alloc_refine_buffer(dims, solvedim: int, device="cuda"):
+    """A 256-byte aligned uint8 view of refine_buffer_size bytes."""
+    import torch
+
+    n = refine_buffer_size(dims, solvedim)
+    raw = torch.empty(n + 256, dtype=torch.uint8, device=device)
+    off = (-raw.data_ptr()) % 256
+    return raw[off:off + n]
+
+
+def gpsv_batch_refine(ds, dl, d, du, dw, x, solvedim: int, steps: int = 1, buffer=None,
+                      reuse_fp32_coefficients: bool = False, stream=None, handle=None,
+                      check: bool = True) -> int:
+    """FP64 solve in place with FP32 sweeps and ``steps`` rounds of FP64
+    residual/correction (``pentadsolver_D_gpsv_batch_refine``)."""
+    _check_arrays((ds, dl, d, du, dw, x))
+    dims = dims_of(x)
+    if buffer is None:
+        buffer = alloc_refine_buffer(dims, solvedim, x.device)
+    st = _typed("pentadsolver_D_gpsv_batch_refine", [_P] * 7 + [_P, _I, _I, _I, _I, _P, _Z, _P])(
+        _hval(handle), *(_ptr(a) for a in (ds, dl, d, du, dw, x)), _dims(dims), len(dims),
+        int(solvedim), int(steps), int(bool(reuse_fp32_coefficients)), _ptr(buffer),
+        buffer.numel() * buffer.element_size(), _stream_ptr(stream, x.device))
+    if check and st != SUCCESS:
+        raise PentadError(st, "gpsv_batch_refine")
+    return st
+
+
+def refine_estimate(buffer, stream=None) -> tuple[float, float]:
+    out = (ctypes.c_double * 2)()
+    st = _typed("pentadsolver_refine_estimate", [_P, _P, _P])(
+        _ptr(buffer), _stream_ptr(stream, buffer.device), out)
+    if st != SUCCESS:
+        raise PentadError(st, "refine estimate")
+    return out[0], out[1]
