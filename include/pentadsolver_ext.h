@@ -52,6 +52,16 @@ EXTERN_C PENTAD_API pentadStatus_t pentadsolver_set_algo(pentadsolver_handle_t h
                                               int dir, const char *algo,
                                               int pcr_lanes);
 
+/* Kernel choice within a family for one direction of this handle, as an
+ * autotuner sets it: "auto" (or NULL), "no-tmem" (skip the Tensor-Memory
+ * kernel), "no-tma" (no TMA kernel at all), "tmem=ST,XST" (its variant with
+ * ST forward and XST read-back stages), "tma=R,ST,XST,SCR" (the older TMA
+ * kernel's variant).  When set, it replaces the PENTA_NO_TMEM / PENTA_NO_TMA /
+ * PENTA_TMEM_VARIANT / PENTA_TMA_VARIANT environment variables for this
+ * handle and direction. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_set_tuning(pentadsolver_handle_t handle,
+                                                           int dir, const char *spec);
+
 /* Kernel family the handle's last solve along `dir` launched, and the exact
  * variant (e.g. "thomas-pcr:tiled S16 P2 R1 x8"). */
 EXTERN_C PENTAD_API const char *pentadsolver_kernel_that_ran_ex(

@@ -60,6 +60,33 @@ bool env_flag(const char *name) {
   return v != nullptr && v[0] == '1';
 }
 
+// Kernel-choice knobs for one solve: the handle's tuning for the direction
+// (pentadsolver_set_tuning: "auto", "no-tmem", "no-tma", "tmem=ST,XST",
+// "tma=R,ST,XST,SCR") when set, else the PENTA_NO_TMEM / PENTA_NO_TMA /
+// PENTA_TMEM_VARIANT / PENTA_TMA_VARIANT environment variables.
+struct Knobs {
+  bool no_tma = false, no_tmem = false;
+  std::string tmem_variant, tma_variant;
+};
+Knobs knobs_from(const std::string &tuning) {
+  Knobs k;
+  if (!tuning.empty()) {
+    if (tuning == "no-tma") k.no_tma = true;
+    else if (tuning == "no-tmem") k.no_tmem = true;
+    else if (tuning.rfind("tmem=", 0) == 0) k.tmem_variant = tuning.substr(5);
+    else if (tuning.rfind("tma=", 0) == 0) {
+      k.no_tmem = true;
+      k.tma_variant = tuning.substr(4);
+    }
+    return k;
+  }
+  k.no_tma = env_flag("PENTA_NO_TMA");
+  k.no_tmem = env_flag("PENTA_NO_TMEM");
+  if (const char *e = std::getenv("PENTA_TMEM_VARIANT")) k.tmem_variant = e;
+  if (const char *e = std::getenv("PENTA_TMA_VARIANT")) k.tma_variant = e;
+  return k;
+}
+
 // ---------------------------------------------------------------------------
 // Contexts
 // ---------------------------------------------------------------------------
@@ -72,6 +99,7 @@ struct Context {
   int forced_lanes[3] = {0, 0, 0};
   std::atomic<const char *> ran[3] = {{kNone}, {kNone}, {kNone}};
   std::string variant[3];
+  std::string tuning[3];  // pentadsolver_set_tuning, per direction ("" = none)
   std::unordered_map<long long, int> occ_cache;  // (variant, n) -> CTAs/SM
 
   bool init() {  // idempotent; needs a usable device
@@ -246,7 +274,7 @@ bool pick_tiled(Context &ctx, const Lines &L, bool contig, int P,
 // deepest ring.
 template <typename F>
 bool pick_tma(Context &ctx, const SolveArgs<F> &a, size_t usable_buf, TmaConfig &out,
-              int &occ_out) {
+              int &occ_out, const std::string &variant) {
   if (!tma_supported<F>(a)) return false;
   // the scratch variants keep (dw2, x2) in the caller's buffer
   // (128-byte aligned: they drop whole 128-byte lines of it from L2)
@@ -254,10 +282,10 @@ bool pick_tma(Context &ctx, const SolveArgs<F> &a, size_t usable_buf, TmaConfig 
                       reinterpret_cast<uintptr_t>(a.scratch) % 128 == 0 &&
                       tma_scratch_bytes<F>(a.L) <= usable_buf;
   const std::vector<TmaConfig> &all = tma_configs<F>();
-  // PENTA_TMA_VARIANT="R,stages,xstages,scratch" restricts the choice (tuning)
+  // "R,stages,xstages,scratch" restricts the choice (tuning)
   int want[4] = {-1, -1, -1, -1};
-  if (const char *e = std::getenv("PENTA_TMA_VARIANT"))
-    std::sscanf(e, "%d,%d,%d,%d", &want[0], &want[1], &want[2], &want[3]);
+  if (!variant.empty())
+    std::sscanf(variant.c_str(), "%d,%d,%d,%d", &want[0], &want[1], &want[2], &want[3]);
   int best = -1, best_score = -1, best_occ = 0;
   for (size_t i = 0; i < all.size(); ++i) {
     const TmaConfig &c = all[i];
@@ -335,15 +363,14 @@ bool pick_tma_contig(Context &ctx, const SolveArgs<F> &a, size_t usable_buf,
 
 // The Tensor-Memory kernel: the first compiled variant of this precision and
 // layout that fits shared memory and runs one CTA per SM.
-// PENTA_TMEM_VARIANT="stages,xstages" restricts the choice (tuning).
+// "stages,xstages" restricts the choice (tuning).
 template <typename F>
 bool pick_tmem(Context &ctx, const SolveArgs<F> &a, bool contig, size_t usable_buf,
-               TmemConfig &out) {
+               TmemConfig &out, const std::string &variant) {
   bool w2s = false;
   if (!tmem_supported<F>(a, contig, usable_buf, w2s)) return false;
   int want[2] = {-1, -1};
-  if (const char *e = std::getenv("PENTA_TMEM_VARIANT"))
-    std::sscanf(e, "%d,%d", &want[0], &want[1]);
+  if (!variant.empty()) std::sscanf(variant.c_str(), "%d,%d", &want[0], &want[1]);
   const std::vector<TmemConfig> &all = tmem_configs<F>();
   for (size_t i = 0; i < all.size(); ++i) {
     const TmemConfig &c = all[i];
@@ -414,6 +441,11 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
   const bool contig = (dir == 0);
   const Algo want = selected_algo(ctx, dir);
   const int lanes = selected_lanes(ctx, dir);
+  Knobs kn;
+  {
+    std::lock_guard<std::mutex> lock(ctx.mu);
+    kn = knobs_from(ctx.tuning[dir]);
+  }
   const bool debug = env_flag("PENTA_DEBUG_LAUNCH");
 
   cudaError_t err = cudaSuccess;
@@ -454,7 +486,7 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
       break;
     case Algo::SharedFact: {  // line 0's coefficients for every line (not checked)
       const size_t usable = buf ? std::min(buf_bytes, buffer_bytes(sh, sizeof(F))) : 0;
-      if (!env_flag("PENTA_NO_TMA") && sf_tmem_supported<F>(a, contig, ctx.smem_optin)) {
+      if (!kn.no_tma && sf_tmem_supported<F>(a, contig, ctx.smem_optin)) {
         int occ;
         const long long key = (1LL << 58) | ((long long)contig << 1) | (sizeof(F) == 8);
         {
@@ -493,10 +525,10 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
     case Algo::Auto:
     default: {
       const int P = (lanes == 1) ? 1 : 2;
-      if (P == 2 && !env_flag("PENTA_NO_TMA") && !env_flag("PENTA_NO_TMEM")) {
+      if (P == 2 && !kn.no_tma && !kn.no_tmem) {
         TmemConfig mc{};
         const size_t usable = std::min(buf_bytes, buffer_bytes(sh, sizeof(F)));
-        if (pick_tmem<F>(ctx, a, contig, usable, mc)) {
+        if (pick_tmem<F>(ctx, a, contig, usable, mc, kn.tmem_variant)) {
           err = launch_tmem<F>(a, mc, ctx.sm_count, stream);
           if (err == cudaSuccess) {
             char vb[96];
@@ -512,7 +544,7 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
           cudaGetLastError();
         }
       }
-      if (contig && P == 2 && !env_flag("PENTA_NO_TMA")) {
+      if (contig && P == 2 && !kn.no_tma) {
         TmaConfig tc{};
         int occ = 0;
         const size_t usable = std::min(buf_bytes, buffer_bytes(sh, sizeof(F)));
@@ -531,11 +563,11 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
           cudaGetLastError();
         }
       }
-      if (!contig && P == 2 && !env_flag("PENTA_NO_TMA")) {
+      if (!contig && P == 2 && !kn.no_tma) {
         TmaConfig tc{};
         int occ = 0;
         const size_t usable = std::min(buf_bytes, buffer_bytes(sh, sizeof(F)));
-        if (pick_tma<F>(ctx, a, usable, tc, occ)) {
+        if (pick_tma<F>(ctx, a, usable, tc, occ, kn.tma_variant)) {
           err = launch_tma<F>(a, tc, occ * ctx.sm_count, stream);
           if (err == cudaSuccess) {
             char buf[96];
@@ -1116,6 +1148,20 @@ extern "C" pentadStatus_t pentadsolver_set_algo(pentadsolver_handle_t h,
   std::lock_guard<std::mutex> lock(ctx->mu);
   ctx->forced[dir] = a;
   ctx->forced_lanes[dir] = pcr_lanes;
+  return PENTAD_STATUS_SUCCESS;
+}
+
+extern "C" pentadStatus_t pentadsolver_set_tuning(pentadsolver_handle_t h, int dir,
+                                                  const char *spec) {
+  if (dir < 0 || dir > 2) return PENTAD_STATUS_INVALID_VALUE;
+  std::string v = spec ? spec : "";
+  if (v == "auto") v.clear();
+  const bool ok = v.empty() || v == "no-tma" || v == "no-tmem" || v.rfind("tmem=", 0) == 0 ||
+                  v.rfind("tma=", 0) == 0;
+  if (!ok) return PENTAD_STATUS_INVALID_VALUE;
+  Context *ctx = penta::resolve(h);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->tuning[dir] = v;
   return PENTAD_STATUS_SUCCESS;
 }
 

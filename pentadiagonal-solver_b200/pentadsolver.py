@@ -414,3 +414,12 @@ def refine_estimate(buffer, stream=None) -> tuple[float, float]:
     if st != SUCCESS:
         raise PentadError(st, "refine estimate")
     return out[0], out[1]
+
+
+def set_tuning(handle, direction: int, spec: str | None) -> None:
+    """pentadsolver_set_tuning: "auto", "no-tmem", "no-tma", "tmem=ST,XST",
+    "tma=R,ST,XST,SCR" for one direction of a handle."""
+    st = _typed("pentadsolver_set_tuning", [_P, _I, ctypes.c_char_p])(
+        _hval(handle), int(direction), None if spec is None else spec.encode())
+    if st != SUCCESS:
+        raise PentadError(st, f"set_tuning({spec!r})")

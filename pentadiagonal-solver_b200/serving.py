@@ -1,0 +1,320 @@
+"""Serving: a continuous-batching request loop over device-resident problems.
+
+Requests (a grid shape, a solve direction, a tolerance) arrive on a clock --
+a Poisson stream in the benchmarks.  The loop
+
+  * admits queued requests first come, first served while their device
+    memory (the request's iterate plus the scratch of the plan that will
+    solve it) fits the HBM budget;
+  * groups admitted requests by (solvedim, precision class) and launches each
+    group as one plan -- one persistent launch for all its grids -- on one of
+    several CUDA streams, so batches overlap on the device and requests that
+    arrive while others run join the next batch as soon as memory frees;
+  * keeps coefficients device-resident (a pool of problems built once) and
+    each request's iterate on the device from admission to completion;
+  * records each request's latency (completion minus arrival) and reports
+    p50/p99 beside throughput.
+
+Precision classes: requests at tolerance >= 1e-10 may use mixed precision
+(FP32 sweeps + FP64 refinement) under the "mixed" policy; tighter ones always
+use plain FP64.  The "sequential" policy is the baseline: each request solved
+alone by one plain FP64 call, in arrival order.
+
+The scheduler (admission, grouping, budget accounting) is independent of the
+GPU: ``Scheduler`` drives an executor object, and the CUDA executor here is
+one implementation of it.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float          # seconds from the start of the trace
+    problem: int            # index into the problem pool
+    solvedim: int
+    tol: float
+    admitted: float = math.nan
+    started: float = math.nan
+    done: float = math.nan
+    batch: int = -1
+
+    @property
+    def mixed_ok(self) -> bool:
+        return self.tol >= 1e-10
+
+
+def log_uniform_dims(rng, lo, hi, ndim=3):
+    return tuple(int(round(math.exp(rng.uniform(math.log(lo), math.log(hi))))) for _ in range(ndim))
+
+
+def make_trace(n_requests: int, rate: float, n_problems: int, seed: int,
+               frac_loose: float = 0.7) -> list[Request]:
+    """Poisson arrivals (exponential gaps, mean 1/rate; rate = inf puts every
+    request at t = 0), uniform problem index, solvedim U{0,1,2}, tolerance
+    1e-10 with probability frac_loose, else 1e-13."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n_requests):
+        if math.isfinite(rate):
+            t += rng.exponential(1.0 / rate)
+        out.append(Request(i, t, int(rng.integers(n_problems)), int(rng.integers(3)),
+                           1e-10 if rng.random() < frac_loose else 1e-13))
+    return out
+
+
+def percentile(values, q):
+    v = sorted(values)
+    if not v:
+        return math.nan
+    k = (len(v) - 1) * q
+    lo, hi = math.floor(k), math.ceil(k)
+    return v[lo] + (v[hi] - v[lo]) * (k - lo)
+
+
+@dataclass
+class Batch:
+    bid: int
+    requests: list
+    key: tuple
+    nbytes: int
+    handle: object = None    # executor's in-flight token
+
+
+class Scheduler:
+    """Admission by budget and continuous batching, driven by a clock.
+
+    The executor provides: ``request_bytes(req)``, ``batch_bytes(reqs, key)``,
+    ``launch(batch) -> token``, ``done(token) -> bool``, ``finish(batch)``,
+    ``now() -> float`` (seconds since start) and ``idle()`` (wait a little).
+    """
+
+    def __init__(self, executor, budget_bytes: float, max_batch: int = 64,
+                 max_in_flight: int = 3, policy: str = "mixed"):
+        self.x = executor
+        self.budget = float(budget_bytes)
+        self.max_batch = max_batch
+        self.max_in_flight = max_in_flight
+        self.policy = policy
+        self.used = 0.0
+        self.peak = 0.0
+        self.batches = 0
+
+    def reserve(self, r: Request) -> float:
+        """Device bytes a request holds from admission to completion."""
+        return self.x.request_bytes(r) + self.x.batch_bytes([r], self.key_of(r))
+
+    def key_of(self, r: Request):
+        if self.policy == "sequential":
+            return ("seq", r.rid)
+        prec = "mixed" if (self.policy == "mixed" and r.mixed_ok) else "f64"
+        return (r.solvedim, prec)
+
+    def run(self, trace: list[Request]) -> list[Request]:
+        pending = sorted(trace, key=lambda r: r.arrival)
+        arrived: list[Request] = []     # queued, not admitted
+        admitted: list[Request] = []    # admitted, not launched
+        in_flight: list[Batch] = []
+        i = 0
+        finished = 0
+        while finished < len(trace):
+            now = self.x.now()
+            while i < len(pending) and pending[i].arrival <= now:
+                arrived.append(pending[i])
+                i += 1
+            # completions free memory first
+            for b in [b for b in in_flight if self.x.done(b.handle)]:
+                t = self.x.now()
+                self.x.finish(b)
+                for r in b.requests:
+                    r.done = t
+                self.used -= b.nbytes
+                in_flight.remove(b)
+                finished += len(b.requests)
+            # admission: first come, first served, while a request's iterate
+            # and its share of plan scratch fit (a lone request larger than
+            # the whole budget still runs, by itself)
+            while arrived:
+                r = arrived[0]
+                need = self.reserve(r)
+                if self.used + need > self.budget and (self.used > 0 or admitted):
+                    break
+                arrived.pop(0)
+                r.admitted = now
+                self.used += need
+                self.peak = max(self.peak, self.used)
+                admitted.append(r)
+            # launch: the group holding the oldest admitted request
+            launched = False
+            while admitted and len(in_flight) < self.max_in_flight:
+                key = self.key_of(admitted[0])
+                group = [r for r in admitted if self.key_of(r) == key][: self.max_batch]
+                t_launch = self.x.now()
+                for r in group:
+                    admitted.remove(r)
+                    r.started = t_launch
+                    r.batch = self.batches
+                b = Batch(self.batches, group, key, sum(self.reserve(r) for r in group))
+                self.batches += 1
+                b.handle = self.x.launch(b)
+                in_flight.append(b)
+                launched = True
+            if not launched:
+                if i < len(pending) and not in_flight and not admitted:
+                    self.x.idle(until=pending[i].arrival)
+                else:
+                    self.x.idle()
+        return trace
+
+
+def report(trace: list[Request]) -> dict:
+    lat = [(r.done - r.arrival) * 1e3 for r in trace]
+    t0 = min(r.arrival for r in trace)
+    t1 = max(r.done for r in trace)
+    return {
+        "requests": len(trace),
+        "solves_per_s": round(len(trace) / (t1 - t0), 1),
+        "p50_ms": round(percentile(lat, 0.5), 3),
+        "p99_ms": round(percentile(lat, 0.99), 3),
+        "mean_ms": round(sum(lat) / len(lat), 3),
+        "makespan_s": round(t1 - t0, 4),
+    }
+
+
+# ---------------------------------------------------------------------------
+# The CUDA executor
+# ---------------------------------------------------------------------------
+class ProblemPool:
+    """Device-resident FP64 problems (coefficients and a right-hand side)
+    with random dominant coefficients as in the 64^3 parity config."""
+
+    def __init__(self, shapes, device="cuda", seed=0):
+        import torch
+
+        self.shapes = [tuple(s) for s in shapes]
+        self.items = []
+        g = torch.Generator(device=device).manual_seed(seed)
+        for dims in self.shapes:
+            shape = tuple(reversed(dims))
+
+            def u(lo, hi):
+                return torch.rand(shape, generator=g, device=device,
+                                  dtype=torch.float64) * (hi - lo) + lo
+
+            ds, dl, du, dw = u(-1, 1), u(-1, 1), u(-1, 1), u(-1, 1)
+            d = ds.abs() + dl.abs() + du.abs() + dw.abs() + u(1, 2)
+            self.items.append({"ds": ds, "dl": dl, "d": d, "du": du, "dw": dw, "b": u(-1, 1)})
+
+    def points(self, i) -> int:
+        return int(math.prod(self.shapes[i]))
+
+    def nbytes(self) -> int:
+        return sum(7 * 8 * self.points(i) for i in range(len(self.shapes)))
+
+
+class CudaExecutor:
+    """Runs batches as plans (or, for the sequential baseline, single calls)."""
+
+    def __init__(self, pool: ProblemPool, refine_steps: int = 1, streams: int = 3,
+                 keep_results: bool = False):
+        import torch
+
+        import pentadsolver as ps
+
+        self.ps = ps
+        self.torch = torch
+        self.pool = pool
+        self.refine_steps = refine_steps
+        self.streams = [torch.cuda.Stream() for _ in range(streams)]
+        self.next_stream = 0
+        self.keep_results = keep_results
+        self.results = {}
+        self.t0 = time.perf_counter()
+        self.handle = ps.Handle()
+
+    def now(self) -> float:
+        return time.perf_counter() - self.t0
+
+    def idle(self, until: float | None = None) -> None:
+        if until is not None:
+            dt = until - self.now()
+            if dt > 2e-4:
+                time.sleep(dt - 1e-4)
+
+    def request_bytes(self, r: Request) -> int:
+        return 8 * self.pool.points(r.problem)   # its iterate
+
+    def batch_bytes(self, reqs, key) -> int:
+        # plan scratch: at most the reference-sized buffer of each grid
+        # (refinement: FP32 copies + residual + saved b + an FP32 buffer)
+        per = 0
+        for r in reqs:
+            n = self.pool.points(r.problem)
+            mixed = key[1] == "mixed" if key[0] != "seq" else False
+            per += n * (20 + 4 + 8 + 36) if mixed else n * 8 * 9
+        return per
+
+    def launch(self, b: Batch):
+        torch, ps = self.torch, self.ps
+        s = self.streams[self.next_stream]
+        self.next_stream = (self.next_stream + 1) % len(self.streams)
+        grids = []
+        with torch.cuda.stream(s):
+            for r in b.requests:
+                p = self.pool.items[r.problem]
+                x = p["b"].clone()
+                grids.append({"ds": p["ds"], "dl": p["dl"], "d": p["d"], "du": p["du"],
+                              "dw": p["dw"], "x": x})
+            if b.key[0] == "seq":
+                r, g = b.requests[0], grids[0]
+                buf = ps.alloc_buffer(ps.dims_of(g["x"]), r.solvedim, torch.float64)
+                ps.gpsv_batch(g["ds"], g["dl"], g["d"], g["du"], g["dw"], g["x"], r.solvedim,
+                              buffer=buf, stream=s, handle=self.handle)
+                plan = buf
+            else:
+                steps = self.refine_steps if b.key[1] == "mixed" else None
+                plan = ps.Plan(grids, b.key[0], refine_steps=steps, handle=self.handle)
+                plan.execute(s)
+            ev = torch.cuda.Event()
+            ev.record(s)
+        if b.key[0] == "seq":
+            ev.synchronize()   # the baseline waits for each call
+        return (ev, plan, grids)
+
+    def done(self, token) -> bool:
+        return token[0].query()
+
+    def finish(self, b: Batch) -> None:
+        ev, plan, grids = b.handle
+        if hasattr(plan, "close"):
+            plan.close()
+        if self.keep_results:
+            for r, g in zip(b.requests, grids):
+                self.results[r.rid] = g["x"]
+        b.handle = None
+
+
+def serve(pool: ProblemPool, trace, policy: str, budget_bytes: float, max_batch: int = 64,
+          refine_steps: int = 1, keep_results: bool = False):
+    """Run a trace in real time; returns (report, executor)."""
+    import copy
+
+    tr = copy.deepcopy(trace)
+    ex = CudaExecutor(pool, refine_steps=refine_steps, keep_results=keep_results)
+    sch = Scheduler(ex, budget_bytes, max_batch=max_batch,
+                    max_in_flight=1 if policy == "sequential" else 3, policy=policy)
+    ex.torch.cuda.synchronize()
+    ex.t0 = time.perf_counter()
+    sch.run(tr)
+    ex.torch.cuda.synchronize()
+    rep = report(tr)
+    rep.update({"policy": policy, "batches": sch.batches,
+                "peak_budget_gb": round(sch.peak / 1e9, 3)})
+    return rep, ex, tr
