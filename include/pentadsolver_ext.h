@@ -96,6 +96,16 @@ EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_buffer_size(
 EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_create(
     pentadsolver_handle_t handle, int elem_bytes, int count, const pentadsolver_grid_t *grids,
     int solvedim, void *buffer, size_t buffer_bytes, int ctas, pentadsolver_plan_t *plan);
+/* The same with the job table and the scratch in separate memory: plans
+ * that never run at the same time (e.g. the x, y and z plans of one ADI
+ * iteration on one stream) may share one scratch region. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_sizes(
+    pentadsolver_handle_t handle, int elem_bytes, int count, const pentadsolver_grid_t *grids,
+    int solvedim, size_t *table_bytes, size_t *scratch_bytes);
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_create_split(
+    pentadsolver_handle_t handle, int elem_bytes, int count, const pentadsolver_grid_t *grids,
+    int solvedim, void *table, size_t table_bytes, void *scratch, size_t scratch_bytes,
+    int ctas, pentadsolver_plan_t *plan);
 EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_execute(pentadsolver_plan_t plan,
                                                               void *stream);
 EXTERN_C PENTAD_API const char *pentadsolver_plan_describe(pentadsolver_plan_t plan);

@@ -1,0 +1,340 @@
+#!/usr/bin/env python3
+"""Measurements of the solver's other workloads, one JSON line each.
+
+  config0  64^3 FP64, random dominant coefficients, x then y then z: time per
+           axis and forward error against the CPU oracle (parity workload).
+  config2  512^3 random dominant coefficients: plain FP64 against FP32 sweeps
+           with 1..3 FP64 refinement steps; time, GB/s (56 B per point and
+           axis for both: the same useful work) and forward error against
+           the FP64 oracle (CPU oracle along y, the plain FP64 GPU solve --
+           itself within 1e-12 of the oracle -- along x and z).
+  config3  96 grids, N_x, N_y, N_z ~ U[32, 384] (seeded), random dominant
+           coefficients, x, y and z each one plan (one persistent launch),
+           the three captured in one CUDA graph; FP64 and FP32 + 1 refinement
+           step; against per-grid single calls.
+  config4  serving: a Poisson stream (2000 requests/s) of grids with per-axis
+           N ~ logU[16, 512] from a device-resident pool, solvedim U{0,1,2},
+           70% at tolerance 1e-10 and 30% at 1e-13, 150 GB budget; p50/p99
+           latency and solves/s for the mixed and FP64 policies and for
+           sequential plain FP64 calls, at that rate and at saturation.
+
+All inputs are synthetic (seeded); times are CUDA-event device times except
+the serving loop (wall clock, as a client sees it).
+
+  python pentadiagonal-solver_b200/bench_configs.py [--configs 0,2,3,4]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import sys
+import time
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parent
+for p in (str(HERE), str(REPO), str(REPO / "tests")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+NAMES = ("ds", "dl", "d", "du", "dw", "x")
+
+
+def peak():
+    try:
+        return float(json.loads((REPO / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+def dev_problem(dims, seed, dtype=None):
+    """Random dominant problem (config-0 distribution) generated on the GPU."""
+    import torch
+
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    shape = tuple(reversed(list(dims)))
+
+    def u(lo, hi):
+        return torch.rand(shape, generator=g, device="cuda", dtype=torch.float64) * (hi - lo) + lo
+
+    ds, dl, du, dw = u(-1, 1), u(-1, 1), u(-1, 1), u(-1, 1)
+    d = ds.abs() + dl.abs() + du.abs() + dw.abs() + u(1, 2)
+    out = {"ds": ds, "dl": dl, "d": d, "du": du, "dw": dw, "x": u(-1, 1)}
+    if dtype is not None:
+        out = {k: v.to(dtype) for k, v in out.items()}
+    return out
+
+
+def timed(fn, reps=3, warmup=1):
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def fwd_err(a, b) -> float:
+    import torch
+
+    a = a.double()
+    b = b.double()
+    return float((a - b).abs().max() / b.abs().max())
+
+
+def config0():
+    import torch
+
+    import fixtures
+    import pentadsolver as ps
+    from oracle import oracle
+
+    dims = (64, 64, 64)
+    co = fixtures.random_dominant(dims, 20240601, np.float64)
+    dv = {k: torch.from_numpy(co[k]).cuda() for k in NAMES}
+    ref = co["x"].copy()
+    per_axis, errs = [], []
+    with ps.Handle() as h:
+        for axis in range(3):
+            x0 = dv["x"].clone()
+            ms = timed(lambda: (dv["x"].copy_(x0), ps.gpsv_batch(*(dv[k] for k in NAMES), axis,
+                                                                  handle=h)))
+            dv["x"].copy_(x0)
+            ps.gpsv_batch(*(dv[k] for k in NAMES), axis, handle=h)
+            oracle.solve(co["ds"], co["dl"], co["d"], co["du"], co["dw"], ref, axis)
+            errs.append(float(np.abs(dv["x"].cpu().numpy() - ref).max() / np.abs(ref).max()))
+            per_axis.append(round(ms * 1e3, 2))
+    return {"config": "config0_64cube_fp64_xyz", "us_per_axis_incl_copy": per_axis,
+            "fwd_err_vs_oracle": errs, "tolerance": 1e-12,
+            "note": "L2-resident parity workload (14 MiB per axis)"}
+
+
+def config2(n=512):
+    import torch
+
+    import pentadsolver as ps
+    from oracle import oracle
+
+    dims = (n, n, n)
+    p = dev_problem(dims, 2)
+    b = p["x"].clone()
+    pts = n ** 3
+    out = {"config": f"config2_{n}cube_precision", "points": pts, "axes": []}
+    with ps.Handle() as h:
+        for axis in range(3):
+            buf = ps.alloc_buffer(list(dims), axis, torch.float64)
+            x64 = b.clone()
+
+            def plain():
+                x64.copy_(b)
+                ps.gpsv_batch(p["ds"], p["dl"], p["d"], p["du"], p["dw"], x64, axis, buffer=buf,
+                              handle=h)
+
+            ms64 = timed(plain)
+            copy_ms = timed(lambda: x64.copy_(b))
+            plain()
+            torch.cuda.synchronize()
+            ref = x64.clone()
+            err_kind = "gpu_fp64"
+            if axis == 1:  # the CPU FP64 oracle on this axis
+                host = {k: p[k].cpu().numpy() for k in ("ds", "dl", "d", "du", "dw")}
+                xr = b.cpu().numpy()
+                oracle.set_threads(__import__("os").cpu_count() or 1)
+                oracle.solve(host["ds"], host["dl"], host["d"], host["du"], host["dw"], xr, axis)
+                ref = torch.from_numpy(xr).cuda()
+                err_kind = "cpu_oracle"
+                del host
+            row = {"axis": axis, "fp64": {"ms": round(ms64 - copy_ms, 4),
+                                          "variant": h.variant_that_ran(0 if axis == 0 else (2 if axis == 2 else 1)),
+                                          "fwd_err": fwd_err(x64, ref)}}
+            del buf
+            rbuf = ps.alloc_refine_buffer(list(dims), axis)
+            xm = b.clone()
+            for steps in (0, 1, 2, 3):
+                def mixed(steps=steps, reuse=True):
+                    xm.copy_(b)
+                    ps.gpsv_batch_refine(p["ds"], p["dl"], p["d"], p["du"], p["dw"], xm, axis,
+                                         steps=steps, buffer=rbuf, reuse_fp32_coefficients=reuse,
+                                         handle=h)
+
+                mixed(reuse=False)   # cast the coefficients once
+                ms = timed(mixed) - copy_ms
+                mixed()
+                torch.cuda.synchronize()
+                dmax, xmax = ps.refine_estimate(rbuf)
+                row[f"fp32_ir{steps}"] = {"ms": round(ms, 4), "fwd_err": fwd_err(xm, ref),
+                                          "estimate": dmax / xmax if xmax else None}
+            # the cast itself (when coefficients change per solve)
+            row["fp32_cast_ms"] = round(timed(lambda: mixed(1, False)) - timed(lambda: mixed(1, True)), 4)
+            del rbuf
+            row["fp64"]["GBps"] = round(56 * pts / (row["fp64"]["ms"] * 1e-3) / 1e9, 1)
+            for s in (1, 2, 3):
+                k = f"fp32_ir{s}"
+                row[k]["GBps_equiv"] = round(56 * pts / (row[k]["ms"] * 1e-3) / 1e9, 1)
+                row[k]["speed_vs_fp64"] = round(row["fp64"]["ms"] / row[k]["ms"], 3)
+            row["fwd_err_reference"] = err_kind
+            out["axes"].append(row)
+            torch.cuda.empty_cache()
+    out["peak_GBps"] = peak()
+    out["target_fwd_err"] = 1e-10
+    return out
+
+
+def config3(n_grids=96, lo=32, hi=384, seed=33):
+    import torch
+
+    import pentadsolver as ps
+
+    rng = np.random.default_rng(seed)
+    dims_list = [tuple(int(v) for v in rng.integers(lo, hi + 1, size=3)) for _ in range(n_grids)]
+    pts = sum(math.prod(d) for d in dims_list)
+    grids = [dev_problem(d, 1000 + i) for i, d in enumerate(dims_list)]
+    rhs = [g["x"].clone() for g in grids]
+    out = {"config": "config3_batched_uneven", "grids": n_grids, "points": pts,
+           "N_range": [lo, hi], "seed": seed}
+
+    def restore():
+        for g, r in zip(grids, rhs):
+            g["x"].copy_(r)
+
+    restore_ms = timed(restore)
+    # FP64 plans, captured together; the three share one scratch region
+    shared = ps.aligned_bytes(max(ps.plan_sizes(grids, a)[1] for a in range(3)))
+    plans = [ps.Plan(grids, axis, scratch=shared) for axis in range(3)]
+    out["fp64_plans"] = [pl.describe() for pl in plans]
+    s = torch.cuda.Stream()
+    restore()
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        for pl in plans:
+            pl.execute(s)
+    ms = timed(lambda: (restore(), graph.replay())) - restore_ms
+    restore()
+    graph.replay()
+    torch.cuda.synchronize()
+    ref = [g["x"].clone() for g in grids]
+    out["fp64_graph_ms_xyz"] = round(ms, 3)
+    out["fp64_GBps"] = round(3 * 56 * pts / (ms * 1e-3) / 1e9, 1)
+    out["fp64_systems_per_s"] = round(sum(3 * math.prod(d) / max(d) for d in dims_list) / (ms * 1e-3))
+    del graph
+    for pl in plans:
+        pl.close()
+    del plans, shared
+    torch.cuda.empty_cache()
+    # sequential single calls (one launch per grid and axis, one stream, one
+    # buffer sized for the largest grid)
+    with ps.Handle() as h:
+        buf = ps.aligned_bytes(max(ps.buffer_size(list(d), 0, 8) for d in dims_list))
+
+        def singles():
+            for g in grids:
+                for axis in range(3):
+                    ps.gpsv_batch(g["ds"], g["dl"], g["d"], g["du"], g["dw"], g["x"], axis,
+                                  buffer=buf, handle=h)
+
+        ms_single = timed(lambda: (restore(), singles())) - restore_ms
+    del buf
+    torch.cuda.empty_cache()
+    out["single_calls_ms_xyz"] = round(ms_single, 3)
+    out["batched_speedup"] = round(ms_single / ms, 3)
+    # FP32 sweeps + 1 refinement step: one refinement plan per axis (its FP32
+    # copies of the coefficients live in its own buffer), each axis captured
+    # in a graph and timed, over the first `ir_grids` grids (device memory)
+    ir_grids = min(n_grids, 48)
+    sub, sub_rhs, sub_ref = grids[:ir_grids], rhs[:ir_grids], ref[:ir_grids]
+    pts_ir = sum(math.prod(d) for d in dims_list[:ir_grids])
+    out["ir1_grids"] = ir_grids
+    try:
+        for g, r in zip(sub, sub_rhs):
+            g["x"].copy_(r)
+        ms_axes = []
+        for axis in range(3):
+            rp = ps.Plan(sub, axis, refine_steps=1)
+            saved = [g["x"].clone() for g in sub]
+
+            def put_back():
+                for g, sv in zip(sub, saved):
+                    g["x"].copy_(sv)
+
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=s):
+                rp.execute(s)
+            ms_axes.append(timed(lambda: (put_back(), graph.replay())) - timed(put_back))
+            put_back()
+            graph.replay()           # leave this axis solved, then the next axis
+            torch.cuda.synchronize()
+            del graph, saved
+            rp.close()
+            del rp
+            torch.cuda.empty_cache()
+        ms_r = sum(ms_axes)
+        out["ir1_ms_xyz"] = round(ms_r, 3)
+        out["ir1_ms_per_axis"] = [round(v, 3) for v in ms_axes]
+        out["ir1_GBps_equiv"] = round(3 * 56 * pts_ir / (ms_r * 1e-3) / 1e9, 1)
+        out["ir1_fwd_err_max_vs_fp64"] = max(fwd_err(g["x"], r) for g, r in zip(sub, sub_ref))
+    except RuntimeError as e:  # device memory
+        out["ir1_error"] = str(e)[:200]
+    out["peak_GBps"] = peak()
+    return out
+
+
+def config4(rate=2000.0, seconds=2.0, n_problems=64, budget=150e9, seed=44):
+    import torch
+
+    import serving
+
+    rng = np.random.default_rng(seed)
+    shapes = [serving.log_uniform_dims(rng, 16, 512) for _ in range(n_problems)]
+    pool = serving.ProblemPool(shapes, seed=seed)
+    torch.cuda.synchronize()
+    out = {"config": "config4_serving", "rate_per_s": rate, "pool_problems": n_problems,
+           "pool_GB": round(pool.nbytes() / 1e9, 2), "budget_GB": budget / 1e9}
+    n_req = int(rate * seconds)
+    for label, r in (("nominal", rate), ("saturated", math.inf)):
+        trace = serving.make_trace(n_req if label == "nominal" else n_req // 2, r, n_problems,
+                                   seed=seed + 1)
+        res = {}
+        for policy in ("mixed", "fp64", "sequential"):
+            rep, ex, _ = serving.serve(pool, trace, policy, budget)
+            res[policy] = rep
+            del ex
+            torch.cuda.empty_cache()
+        res["speedup_mixed_vs_sequential"] = round(res["mixed"]["solves_per_s"] /
+                                                   res["sequential"]["solves_per_s"], 3)
+        res["speedup_fp64_vs_sequential"] = round(res["fp64"]["solves_per_s"] /
+                                                  res["sequential"]["solves_per_s"], 3)
+        out[label] = res
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--configs", default="0,2,3,4")
+    ap.add_argument("--n2", type=int, default=512, help="grid edge of config 2")
+    ap.add_argument("--grids3", type=int, default=96)
+    ap.add_argument("--seconds4", type=float, default=2.0)
+    args = ap.parse_args()
+    want = {c.strip() for c in args.configs.split(",")}
+    runs = {"0": config0, "2": lambda: config2(args.n2), "3": lambda: config3(args.grids3),
+            "4": lambda: config4(seconds=args.seconds4)}
+    for c in ("0", "2", "3", "4"):
+        if c in want:
+            t0 = time.time()
+            res = runs[c]()
+            res["wall_s"] = round(time.time() - t0, 1)
+            print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -639,29 +639,37 @@ struct Plan {
   Context *ctx = nullptr;
   int elem = 8, solvedim = 0;
   bool contig = false, w2s = false, discard = false;
-  unsigned char *buffer = nullptr;
+  unsigned char *table = nullptr, *scratch = nullptr;
   int n_jobs = 0, total_tiles = 0, ctas = 0;
+  struct Group {  // one batched launch: jobs [first, first + count) of the table
+    int first, count, tiles;
+    bool w2s;
+  };
+  std::vector<Group> groups;
   std::vector<PlanSingle> singles;
   std::string desc;
   // mixed-precision refinement over the same grids (refine plans only)
   bool refine = false;
   int steps = 0, chunks = 0;
-  RefineGrid *table = nullptr;   // device
+  RefineGrid *rtable = nullptr;  // device
   double *est = nullptr;         // device [count][2]
   int count = 0;
   Plan *fp32 = nullptr;          // the FP32 plan over the cast copies
   ~Plan() { delete fp32; }
 };
 
-// Buffer layout of a plan: [job table][scratch of each batched grid][buffer
-// of each grid solved alone], every region 256-byte aligned.  `order` gets
-// the batched grids, heaviest lines first (tiles are dealt round-robin to the
-// consumer warps, so this balances the tail).
+// Memory of a plan: a job table (table_bytes) and scratch (scratch_bytes:
+// each batched grid's region, then each alone-solved grid's buffer), every
+// region 256-byte aligned; `offs` are relative to the scratch.  In one
+// buffer the table comes first.  `order` gets the batched grids, heaviest
+// lines first (tiles are dealt round-robin to the consumer warps, so this
+// balances the tail).
 template <typename F>
 pentadStatus_t plan_layout(Context &ctx, int count, const pentadsolver_grid_t *grids,
                            int solvedim, std::vector<int> &order, std::vector<size_t> &offs,
-                           std::vector<PlanSingle> &singles, bool &w2s, size_t &total,
-                           const char **why) {
+                           std::vector<PlanSingle> &singles, bool &w2s, size_t &table_bytes,
+                           size_t &scratch_bytes, const char **why,
+                           std::vector<char> *grid_w2s = nullptr) {
   if (count < 1 || grids == nullptr) {
     *why = "no grids";
     return PENTAD_STATUS_INVALID_VALUE;
@@ -692,14 +700,20 @@ pentadStatus_t plan_layout(Context &ctx, int count, const pentadsolver_grid_t *g
       order.push_back(i);
       w2s = w2s || need_w2s[i];
     }
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int a, int b) { return shapes[a].L.n > shapes[b].L.n; });
-  size_t off = round256(order.size() * tmem_job_bytes<F>());
+  // two job groups, one per factor mode (du2 and dw2 in TMEM; du2 alone),
+  // each heaviest lines first
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    if (need_w2s[a] != need_w2s[b]) return need_w2s[a] < need_w2s[b];
+    return shapes[a].L.n > shapes[b].L.n;
+  });
+  table_bytes = round256(order.size() * tmem_job_bytes<F>());
+  size_t off = 0;
   offs.assign(count, 0);
   for (int i : order) {
     offs[i] = off;
-    off += round256(tmem_scratch_bytes<F>(shapes[i].L, contig, w2s));
+    off += round256(tmem_scratch_bytes<F>(shapes[i].L, contig, need_w2s[i]));
   }
+  if (grid_w2s) *grid_w2s = need_w2s;
   singles.clear();
   for (int i = 0; i < count; ++i)
     if (!ok[i]) {
@@ -707,14 +721,14 @@ pentadStatus_t plan_layout(Context &ctx, int count, const pentadsolver_grid_t *g
       singles.push_back(PlanSingle{grids[i], off, b});
       off += round256(b);
     }
-  total = off;
+  scratch_bytes = off;
   return PENTAD_STATUS_SUCCESS;
 }
 
 template <typename F>
 pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *grids,
-                          int solvedim, void *buffer, size_t buffer_bytes_given, int ctas,
-                          Plan *&out, const char **why) {
+                          int solvedim, void *table_buf, size_t table_given, void *scratch_buf,
+                          size_t scratch_given, int ctas, Plan *&out, const char **why) {
   if (!ctx.init()) {
     *why = "no usable CUDA device";
     return PENTAD_STATUS_NOT_INITIALIZED;
@@ -723,16 +737,22 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
   std::vector<size_t> offs;
   std::vector<PlanSingle> singles;
   bool w2s = false;
-  size_t total = 0;
-  pentadStatus_t st =
-      plan_layout<F>(ctx, count, grids, solvedim, order, offs, singles, w2s, total, why);
+  size_t table_bytes = 0, scratch_bytes = 0;
+  std::vector<char> gw2s;
+  pentadStatus_t st = plan_layout<F>(ctx, count, grids, solvedim, order, offs, singles, w2s,
+                                     table_bytes, scratch_bytes, why, &gw2s);
   if (st != PENTAD_STATUS_SUCCESS) return st;
-  if (buffer == nullptr || buffer_bytes_given < total ||
-      reinterpret_cast<uintptr_t>(buffer) % 256 != 0) {
-    *why = "the plan needs a 256-byte aligned buffer of pentadsolver_plan_buffer_size bytes";
+  if ((table_bytes > 0 && (table_buf == nullptr || table_given < table_bytes ||
+                           reinterpret_cast<uintptr_t>(table_buf) % 256 != 0)) ||
+      (scratch_bytes > 0 && (scratch_buf == nullptr || scratch_given < scratch_bytes ||
+                             reinterpret_cast<uintptr_t>(scratch_buf) % 256 != 0))) {
+    *why = "the plan needs 256-byte aligned memory of the sizes pentadsolver_plan_buffer_size "
+           "(or pentadsolver_plan_sizes) gives";
     return PENTAD_STATUS_INVALID_VALUE;
   }
-  unsigned char *base = static_cast<unsigned char *>(buffer);
+  unsigned char *base = static_cast<unsigned char *>(scratch_buf);
+  unsigned char *table = static_cast<unsigned char *>(table_buf);
+  std::vector<Plan::Group> groups;
   const bool contig = solvedim == 0;
   int total_tiles = 0;
   if (!order.empty()) {
@@ -754,13 +774,25 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
       *why = "host memory for the job table";
       return PENTAD_STATUS_ALLOC_FAILED;
     }
-    if (!tmem_fill_jobs<F>(args.data(), (int)args.size(), contig, w2s, base, host,
-                           job_offs.data(), &total_tiles)) {
-      std::free(host);
-      *why = "tensor map encoding failed";
-      return PENTAD_STATUS_INTERNAL_ERROR;
+    // fill each factor-mode group as its own tile list
+    size_t first = 0;
+    while (first < order.size()) {
+      size_t last = first;
+      while (last < order.size() && gw2s[order[last]] == gw2s[order[first]]) ++last;
+      int tiles = 0;
+      if (!tmem_fill_jobs<F>(args.data() + first, (int)(last - first), contig,
+                             gw2s[order[first]] != 0, base,
+                             static_cast<unsigned char *>(host) + first * jb,
+                             job_offs.data() + first, &tiles)) {
+        std::free(host);
+        *why = "tensor map encoding failed";
+        return PENTAD_STATUS_INTERNAL_ERROR;
+      }
+      groups.push_back({(int)first, (int)(last - first), tiles, gw2s[order[first]] != 0});
+      total_tiles += tiles;
+      first = last;
     }
-    const cudaError_t e = cudaMemcpy(base, host, order.size() * jb, cudaMemcpyHostToDevice);
+    const cudaError_t e = cudaMemcpy(table, host, order.size() * jb, cudaMemcpyHostToDevice);
     std::free(host);
     if (e != cudaSuccess) {
       cudaGetLastError();
@@ -775,15 +807,17 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
   p->contig = contig;
   p->w2s = w2s;
   p->discard = true;  // every region is 256-byte aligned
-  p->buffer = base;
+  p->table = table;
+  p->scratch = base;
   p->n_jobs = (int)order.size();
   p->total_tiles = total_tiles;
+  p->groups = groups;
   p->ctas = (ctas > 0 && ctas < ctx.sm_count) ? ctas : ctx.sm_count;
   p->singles = singles;
   char d[160];
-  std::snprintf(d, sizeof d, "tmem-batch %s grids=%d tiles=%d%s ctas=%d alone=%d",
-                sizeof(F) == 8 ? "f64" : "f32", p->n_jobs, total_tiles, w2s ? " w2s" : "",
-                p->ctas, (int)singles.size());
+  std::snprintf(d, sizeof d, "tmem-batch %s grids=%d tiles=%d launches=%d%s ctas=%d alone=%d",
+                sizeof(F) == 8 ? "f64" : "f32", p->n_jobs, total_tiles, (int)groups.size(),
+                w2s ? " w2s" : "", p->ctas, (int)singles.size());
   p->desc = d;
   out = p;
   return PENTAD_STATUS_SUCCESS;
@@ -793,9 +827,10 @@ template <typename F> pentadStatus_t plan_run(Plan &p, cudaStream_t stream) {
   Context &ctx = *p.ctx;
   int *status = device_status_word(ctx.device);
   if (status == nullptr) return PENTAD_STATUS_INTERNAL_ERROR;
-  if (p.n_jobs > 0) {
-    const cudaError_t e = launch_tmem_batch<F>(p.buffer, p.n_jobs, p.total_tiles, p.contig,
-                                               p.w2s, p.discard, p.ctas, status, stream);
+  for (const Plan::Group &g : p.groups) {
+    const cudaError_t e =
+        launch_tmem_batch<F>(p.table + g.first * tmem_job_bytes<F>(), g.count, g.tiles,
+                             p.contig, g.w2s, p.discard, p.ctas, status, stream);
     if (e != cudaSuccess) {
       cudaGetLastError();
       return PENTAD_STATUS_EXECUTION_FAILED;
@@ -807,7 +842,7 @@ template <typename F> pentadStatus_t plan_run(Plan &p, cudaStream_t stream) {
         solve<F>(ctx, static_cast<const F *>(s.g.ds), static_cast<const F *>(s.g.dl),
                  static_cast<const F *>(s.g.d), static_cast<const F *>(s.g.du),
                  static_cast<const F *>(s.g.dw), static_cast<F *>(s.g.x), s.g.dims, s.g.ndim,
-                 p.solvedim, p.buffer + s.offset, s.bytes, stream, &why);
+                 p.solvedim, p.scratch + s.offset, s.bytes, stream, &why);
     if (st != PENTAD_STATUS_SUCCESS) return st;
   }
   return PENTAD_STATUS_SUCCESS;
@@ -1215,13 +1250,34 @@ extern "C" pentadStatus_t pentadsolver_plan_buffer_size(pentadsolver_handle_t h,
   std::vector<penta::PlanSingle> singles;
   bool w2s = false;
   const char *why = "";
+  size_t tb = 0, sb = 0;
   pentadStatus_t st =
       elem_bytes == 8
           ? penta::plan_layout<double>(*ctx, count, grids, solvedim, order, offs, singles, w2s,
-                                       *bytes, &why)
+                                       tb, sb, &why)
           : penta::plan_layout<float>(*ctx, count, grids, solvedim, order, offs, singles, w2s,
-                                      *bytes, &why);
+                                      tb, sb, &why);
+  *bytes = tb + sb;
   return st;
+}
+
+extern "C" pentadStatus_t pentadsolver_plan_sizes(pentadsolver_handle_t h, int elem_bytes,
+                                                  int count, const pentadsolver_grid_t *grids,
+                                                  int solvedim, size_t *table_bytes,
+                                                  size_t *scratch_bytes) {
+  if (table_bytes == nullptr || scratch_bytes == nullptr || (elem_bytes != 4 && elem_bytes != 8))
+    return PENTAD_STATUS_INVALID_VALUE;
+  Context *ctx = penta::resolve(h);
+  std::vector<int> order;
+  std::vector<size_t> offs;
+  std::vector<penta::PlanSingle> singles;
+  bool w2s = false;
+  const char *why = "";
+  return elem_bytes == 8
+             ? penta::plan_layout<double>(*ctx, count, grids, solvedim, order, offs, singles,
+                                          w2s, *table_bytes, *scratch_bytes, &why)
+             : penta::plan_layout<float>(*ctx, count, grids, solvedim, order, offs, singles, w2s,
+                                         *table_bytes, *scratch_bytes, &why);
 }
 
 extern "C" pentadStatus_t pentadsolver_plan_create(pentadsolver_handle_t h, int elem_bytes,
@@ -1231,15 +1287,30 @@ extern "C" pentadStatus_t pentadsolver_plan_create(pentadsolver_handle_t h, int 
                                                    pentadsolver_plan_t *plan) {
   if (plan == nullptr || (elem_bytes != 4 && elem_bytes != 8)) return PENTAD_STATUS_INVALID_VALUE;
   *plan = nullptr;
+  size_t tb = 0, sb = 0;
+  pentadStatus_t st = pentadsolver_plan_sizes(h, elem_bytes, count, grids, solvedim, &tb, &sb);
+  if (st != PENTAD_STATUS_SUCCESS) return st;
+  if (buffer == nullptr || buffer_bytes < tb + sb) return PENTAD_STATUS_INVALID_VALUE;
+  unsigned char *b = static_cast<unsigned char *>(buffer);
+  return pentadsolver_plan_create_split(h, elem_bytes, count, grids, solvedim, b, tb, b + tb,
+                                        buffer_bytes - tb, ctas, plan);
+}
+
+extern "C" pentadStatus_t pentadsolver_plan_create_split(
+    pentadsolver_handle_t h, int elem_bytes, int count, const pentadsolver_grid_t *grids,
+    int solvedim, void *table, size_t table_bytes, void *scratch, size_t scratch_bytes, int ctas,
+    pentadsolver_plan_t *plan) {
+  if (plan == nullptr || (elem_bytes != 4 && elem_bytes != 8)) return PENTAD_STATUS_INVALID_VALUE;
+  *plan = nullptr;
   Context *ctx = penta::resolve(h);
   penta::Plan *p = nullptr;
   const char *why = "";
   pentadStatus_t st =
       elem_bytes == 8
-          ? penta::plan_build<double>(*ctx, count, grids, solvedim, buffer, buffer_bytes, ctas,
-                                      p, &why)
-          : penta::plan_build<float>(*ctx, count, grids, solvedim, buffer, buffer_bytes, ctas,
-                                     p, &why);
+          ? penta::plan_build<double>(*ctx, count, grids, solvedim, table, table_bytes, scratch,
+                                      scratch_bytes, ctas, p, &why)
+          : penta::plan_build<float>(*ctx, count, grids, solvedim, table, table_bytes, scratch,
+                                     scratch_bytes, ctas, p, &why);
   if (st != PENTAD_STATUS_SUCCESS) {
     if (penta::env_flag("PENTA_DEBUG_LAUNCH")) std::fprintf(stderr, "[penta] plan: %s\n", why);
     return st;
@@ -1258,7 +1329,7 @@ extern "C" pentadStatus_t pentadsolver_plan_execute(pentadsolver_plan_t plan, vo
   auto step = [&](penta::RefineStep k) {
     penta::RefineGrid none;
     std::memset(&none, 0, sizeof(none));
-    return penta::launch_refine_step(k, none, p.table, p.count, p.chunks, s) == cudaSuccess;
+    return penta::launch_refine_step(k, none, p.rtable, p.count, p.chunks, s) == cudaSuccess;
   };
   pentadStatus_t st;
   if (!step(penta::RefineStep::PrepareCast)) return PENTAD_STATUS_EXECUTION_FAILED;
@@ -1370,8 +1441,12 @@ extern "C" pentadStatus_t pentadsolver_refine_plan_create(pentadsolver_handle_t 
   std::vector<pentadsolver_grid_t> g32;
   penta::refine_fp32_grids(count, grids, shapes, goffs, base, g32);
   penta::Plan *fp32 = nullptr;
-  st = penta::plan_build<float>(*ctx, count, g32.data(), solvedim, base + fp32_off,
-                                buffer_bytes - fp32_off, ctas, fp32, &why);
+  size_t tb = 0, sb = 0;
+  st = pentadsolver_plan_sizes(h, 4, count, g32.data(), solvedim, &tb, &sb);
+  if (st != PENTAD_STATUS_SUCCESS) return st;
+  st = penta::plan_build<float>(*ctx, count, g32.data(), solvedim, base + fp32_off, tb,
+                                base + fp32_off + tb, buffer_bytes - fp32_off - tb, ctas, fp32,
+                                &why);
   if (st != PENTAD_STATUS_SUCCESS) return st;
   // the grid table of the FP64 steps
   std::vector<penta::RefineGrid> table(count);
@@ -1406,7 +1481,7 @@ extern "C" pentadStatus_t pentadsolver_refine_plan_create(pentadsolver_handle_t 
   p->refine = true;
   p->steps = steps;
   p->chunks = chunks;
-  p->table = reinterpret_cast<penta::RefineGrid *>(base);
+  p->rtable = reinterpret_cast<penta::RefineGrid *>(base);
   p->est = est;
   p->count = count;
   p->fp32 = fp32;

@@ -234,6 +234,11 @@ __device__ __forceinline__ void tensormap_acquire(const void *map) {
                : "memory");
 }
 
+// Bring a tensor map into the TMA unit's descriptor cache ahead of use.
+__device__ __forceinline__ void tensormap_prefetch(const void *map) {
+  asm volatile("prefetch.tensormap [%0];\n" ::"l"(map) : "memory");
+}
+
 template <typename F> struct Vec2;
 template <> struct Vec2<double> { using T = double2; };
 template <> struct Vec2<float> { using T = float2; };

@@ -179,13 +179,31 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
       return &job1;
     }
   };
-  auto tile_coords = [&](const TmemJob<F> *J, int tile, int &c0, int &c2) {
+  // a job's geometry, kept in registers while a warp stays on that job
+  struct Geo {
+    const TmemJob<F> *J;
+    F *x, *scratch;
+    int n, mt, inner, tpr, n_sys, tile_base, tma;
+  };
+  auto load_geo = [&](const TmemJob<F> *J, Geo &g) {
+    g.J = J;
+    g.x = J->x;
+    g.scratch = J->scratch;
+    g.n = J->n;
+    g.mt = J->mt;
+    g.inner = J->inner;
+    g.tpr = J->tpr;
+    g.n_sys = J->n_sys;
+    g.tile_base = J->tile_base;
+    g.tma = J->tma;
+  };
+  auto tile_coords = [&](const Geo &g, int tile, int &c0, int &c2) {
     if (CONTIG) {
       c0 = tile * TS;  // first line
       c2 = 0;
     } else {
-      c2 = tile / J->tpr;  // run
-      c0 = (tile - c2 * J->tpr) * TS;
+      c2 = tile / g.tpr;  // run
+      c0 = (tile - c2 * g.tpr) * TS;
     }
   };
 
@@ -194,18 +212,28 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   // all lanes copy elements of a misaligned grid.  full[] counts 32 arrivals.
   if (warp >= NCONS) {
     int slot = 0, use = 0, cursor = 0, fenced = -1;
+    Geo JG;
+    load_geo(job_of(gw, cursor), JG);
     for (int ti = 0; ti < my_tiles; ++ti) {
       const int t = gw + ti * tw;
       const TmemJob<F> *J = job_of(t, cursor);
-      const bool tma = J->tma != 0;
-      if (BATCH && tma && cursor != fenced) {  // host-written maps: acquire them once
-        if (lane == 0)
-          for (int q = 0; q < 6; ++q) tensormap_acquire(&J->maps[q]);
+      if (J != JG.J) load_geo(J, JG);
+      const bool tma = JG.tma != 0;
+      if (BATCH && cursor != fenced) {  // a new grid: its maps, and the next grid's
+        if (lane == 0) {
+          if (tma)
+            for (int q = 0; q < 6; ++q) {
+              tensormap_acquire(&J->maps[q]);  // host-written: acquire once
+              tensormap_prefetch(&J->maps[q]);
+            }
+          if (cursor + 1 < n_jobs && jobs[cursor + 1].tma)
+            for (int q = 0; q < 6; ++q) tensormap_prefetch(&jobs[cursor + 1].maps[q]);
+        }
         fenced = cursor;
       }
       int c0, c2;
-      tile_coords(J, t - J->tile_base, c0, c2);
-      const int n = J->n, mt = J->mt, n_stages = mt / R, inner = J->inner;
+      tile_coords(JG, t - JG.tile_base, c0, c2);
+      const int n = JG.n, mt = JG.mt, n_stages = mt / R, inner = JG.inner;
       for (int g = 0; g < n_stages; ++g) {
         // lane 0 waits for the slot (the others park in the shuffle, issuing
         // nothing) and reads the stop flag for the warp
@@ -264,7 +292,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
             bool valid = row < n;
             long long off;
             if (CONTIG) {
-              valid = valid && c0 + s < J->n_sys;
+              valid = valid && c0 + s < JG.n_sys;
               off = (long long)(c0 + s) * n + row;
             } else {
               valid = valid && c0 + s < inner;
@@ -307,21 +335,24 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
 
   int slot = 0, r_slot = 0, o_buf = 0, cursor = 0;
   unsigned phase = 0, r_phase = 0;
+  Geo JG;
+  load_geo(job_of(gw, cursor), JG);
   long long r_issued = 0, r_consumed = 0;
   bool bad = false, timed_out = false;
 
   for (int ti = 0; ti < my_tiles && !timed_out; ++ti) {
     const int t = gw + ti * tw;
     const TmemJob<F> *J = job_of(t, cursor);
-    const int tile = t - J->tile_base;
+    if (J != JG.J) load_geo(J, JG);
+    const int tile = t - JG.tile_base;
     int c0, c2;
-    tile_coords(J, tile, c0, c2);
-    const int n = J->n, mt = J->mt, inner = J->inner;
+    tile_coords(JG, tile, c0, c2);
+    const int n = JG.n, mt = JG.mt, inner = JG.inner;
     const int n_stages = mt / R;
     const int nvp = part ? 2 * mt - n : 0;  // this half's virtual rows
-    const int count = CONTIG ? min(TS, J->n_sys - c0) : min(TS, inner - c0);
+    const int count = CONTIG ? min(TS, JG.n_sys - c0) : min(TS, inner - c0);
     const bool active = sys < count;
-    F *const x2t = J->scratch + (long long)tile * 2 * mt * TS * PW;  // [2][m][16][PW]
+    F *const x2t = JG.scratch + (long long)tile * 2 * mt * TS * PW;  // [2][m][16][PW]
     F *const x2w = x2t + (part * mt * TS + sys) * PW;                // row k at + k * 16 PW
 
     // ------------------------------ forward ---------------------------------
@@ -479,9 +510,9 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         xb = xa;
         xa = xk[r];
       }
-      if (CONTIG && !J->tma) {  // misaligned grid: each lane writes its own rows
+      if (CONTIG && !JG.tma) {  // misaligned grid: each lane writes its own rows
         if (active) {
-          F *const p = J->x + (long long)(c0 + sys) * n;
+          F *const p = JG.x + (long long)(c0 + sys) * n;
           const int row0 = part ? (mt + s * R) : (mt - 1 - s * R);
 #pragma unroll
           for (int r = 0; r < R; ++r) {
@@ -505,7 +536,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         // the upper half runs towards row 0, the lower half towards row n - 1
         const int row0 = part ? (mt + s * R) : (mt - 1 - s * R);
         const long long step = part ? (long long)inner : -(long long)inner;
-        F *const p = J->x + (long long)c2 * inner * n + c0 + sys + (long long)row0 * inner;
+        F *const p = JG.x + (long long)c2 * inner * n + c0 + sys + (long long)row0 * inner;
         if (part == 0 || mt + (s + 1) * R <= n) {
 #pragma unroll
           for (int r = 0; r < R; ++r) p[r * step] = xk[r];

@@ -292,7 +292,7 @@ class Plan:
     tensors and owns its buffer; execute() is capturable in a CUDA graph."""
 
     def __init__(self, grids, solvedim: int, refine_steps: int | None = None, ctas: int = 0,
-                 handle=None):
+                 handle=None, scratch=None):
         import torch
 
         self.grids = list(grids)
@@ -317,10 +317,31 @@ class Plan:
         if st != SUCCESS:
             raise PentadError(st, "plan buffer size")
         self.buffer_bytes = max(int(size.value), 256)
-        self.buffer = torch.empty(self.buffer_bytes + 256, dtype=torch.uint8, device=self.device)
-        off = (-self.buffer.data_ptr()) % 256
-        self._buf = self.buffer[off:off + self.buffer_bytes]
+        if scratch is None or self.refine:
+            self.buffer = torch.empty(self.buffer_bytes + 256, dtype=torch.uint8,
+                                      device=self.device)
+            off = (-self.buffer.data_ptr()) % 256
+            self._buf = self.buffer[off:off + self.buffer_bytes]
         self._plan = _P(None)
+        if scratch is not None and not self.refine:
+            # job table in its own small buffer, scratch shared with other
+            # plans that never run at the same time
+            tb, sb = plan_sizes(self.grids, self.solvedim, handle)
+            if scratch.numel() * scratch.element_size() < sb or scratch.data_ptr() % 256:
+                raise ValueError(f"scratch needs {sb} bytes, 256-byte aligned")
+            self.scratch = scratch
+            self.buffer = torch.empty(tb + 512, dtype=torch.uint8, device=self.device)
+            off = (-self.buffer.data_ptr()) % 256
+            self._buf = self.buffer[off:off + max(tb, 256)]
+            st = _typed("pentadsolver_plan_create_split",
+                        [_P, _I, _I, ctypes.POINTER(GridDesc), _I, _P, _Z, _P, _Z, _I,
+                         ctypes.POINTER(_P)])(
+                _hval(handle), eb, n, self._descs, self.solvedim, _ptr(self._buf), tb,
+                _ptr(scratch), scratch.numel() * scratch.element_size(), int(ctas),
+                ctypes.byref(self._plan))
+            if st != SUCCESS:
+                raise PentadError(st, "plan create")
+            return
         if self.refine:
             st = _typed("pentadsolver_refine_plan_create",
                         [_P, _I, ctypes.POINTER(GridDesc), _I, _I, _P, _Z, _I, ctypes.POINTER(_P)])(
@@ -423,3 +444,25 @@ def set_tuning(handle, direction: int, spec: str | None) -> None:
         _hval(handle), int(direction), None if spec is None else spec.encode())
     if st != SUCCESS:
         raise PentadError(st, f"set_tuning({spec!r})")
+
+
+def plan_sizes(grids, solvedim: int, handle=None) -> tuple[int, int]:
+    """(job table bytes, scratch bytes) of a plan over these grids."""
+    descs = _grid_descs(grids)
+    tb, sb = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    st = _typed("pentadsolver_plan_sizes",
+                [_P, _I, _I, ctypes.POINTER(GridDesc), _I, ctypes.POINTER(_Z), ctypes.POINTER(_Z)])(
+        _hval(handle), grids[0]["x"].element_size(), len(grids), descs, int(solvedim),
+        ctypes.byref(tb), ctypes.byref(sb))
+    if st != SUCCESS:
+        raise PentadError(st, "plan sizes")
+    return int(tb.value), int(sb.value)
+
+
+def aligned_bytes(n: int, device="cuda"):
+    """A 256-byte aligned uint8 view of n bytes."""
+    import torch
+
+    raw = torch.empty(n + 256, dtype=torch.uint8, device=device)
+    off = (-raw.data_ptr()) % 256
+    return raw[off:off + n]

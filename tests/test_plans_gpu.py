@@ -61,7 +61,9 @@ def test_plan_graph_capture_and_replay(cuda):
     probs = [fixtures.random_dominant(dims, 70 + i, np.float64) for i, dims in enumerate(dims_list)]
     devs = [to_dev(co) for co in probs]
     rhs0 = [dv["x"].clone() for dv in devs]
-    plans = [ps.Plan(devs, axis) for axis in range(3)]
+    # the three plans share one scratch region (they never run at once)
+    shared = ps.aligned_bytes(max(ps.plan_sizes(devs, a)[1] for a in range(3)))
+    plans = [ps.Plan(devs, axis, scratch=shared) for axis in range(3)]
     # eager reference
     for p in plans:
         p.execute()
