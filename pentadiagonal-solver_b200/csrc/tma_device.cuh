@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <mutex>
 
 #include "penta_device.cuh"
@@ -145,6 +146,17 @@ template <int N> __device__ __forceinline__ void bulk_wait_read() {
 // Wait until at most N committed store groups are incomplete.
 template <int N> __device__ __forceinline__ void bulk_wait() {
   asm volatile("cp.async.bulk.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// A progress word in shared memory, published by one warp and polled by another.
+__device__ __forceinline__ int ld_acquire_shared(const int *p) {
+  int v;
+  asm volatile("ld.acquire.cta.shared::cta.b32 %0, [%1];\n" : "=r"(v) : "r"(smem_u32(p)) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_shared(int *p, int v) {
+  asm volatile("st.release.cta.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(p)), "r"(v)
+               : "memory");
 }
 
 __device__ __forceinline__ void discard_l2_line(const void *p) {

@@ -64,7 +64,7 @@ template <typename F, int R, int STAGES, int XST, bool SCR>
 __global__ void __launch_bounds__(64, 1)
 tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
                    F *__restrict__ scratch, int n, int inner, int tiles_per_run,
-                   int n_tiles, int *__restrict__ status_word, int dbg) {
+                   int n_tiles, int *__restrict__ status_word) {
   using G = TmaGeom<F, R, STAGES, XST, SCR>;
   using V2 = typename Vec2<F>::T;
   constexpr int SE = G::SE, XE = G::XE, FW = G::FW;
@@ -181,13 +181,12 @@ tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
       for (int r = 0; r < R; ++r)
 #pragma unroll
         for (int q = 0; q < 6; ++q) a[r][q] = v[r * vs + q * 2 * R * TS];
-      const int my_slot = slot;
-      if (!(dbg & 1)) {
+      {
         // The refill is an async-proxy write: order these generic-proxy reads
         // before it, or a refill can land under a load still in flight.
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[my_slot]);
+        if (lane == 0) mbar_arrive(&empty[slot]);
       }
       if (++slot == STAGES) { slot = 0; phase ^= 1u; }
       if (active) {
@@ -237,10 +236,6 @@ tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
           }
         }
       }
-      if (dbg & 1) {
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[my_slot]);
-      }
     }
     if (timed_out) break;
     bad |= !(isfinite(c.u1) && isfinite(c.u2) && isfinite(c.w1) &&
@@ -280,8 +275,7 @@ tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
           for (int r = 0; r < R; ++r) {
             if (s * R + r < my_rows) {
               if constexpr (sizeof(F) == 8) {
-                if (dbg & 2) cp_async_cg<16>(dst + r * 64, sg + o);
-                else cp_async_ca<16>(dst + r * 64, sg + o);
+                cp_async_ca<16>(dst + r * 64, sg + o);
               } else {
                 cp_async_ca<2 * sizeof(F)>(dst + r * 64, sg + o);
               }
@@ -329,7 +323,7 @@ tma_strided_kernel(const __grid_constant__ TmaMaps maps, F *__restrict__ x,
         // Each lane of a half drops one of the half's 2 x R lines; a line
         // holds 8 lanes' values, so every lane's copy must have landed first.
         __syncwarp();
-        if (!(dbg & 4) && active) {
+        if (active) {
           // a scratch row (16 pairs) is LPR 128-byte lines; lane sys drops
           // line h of the stage's r-th row
           constexpr int LPR = sizeof(F) / 4;
@@ -699,10 +693,8 @@ cudaError_t tma_launch(const SolveArgs<F> &a, int grid, cudaStream_t stream) {
   const int tiles_per_run = (inner + TS - 1) / TS;
   const int n_tiles = (int)(a.L.n_sys / a.L.inner) * tiles_per_run;
   if (grid <= 0 || grid > n_tiles) grid = n_tiles;
-  int dbg = 0;
-  if (const char *e = std::getenv("PENTA_TMA_DEBUG")) dbg = std::atoi(e);
   kern<<<grid, 64, smem, stream>>>(maps, a.x, static_cast<F *>(a.scratch), n,
-                                   inner, tiles_per_run, n_tiles, a.status, dbg);
+                                   inner, tiles_per_run, n_tiles, a.status);
   return cudaGetLastError();
 }
 

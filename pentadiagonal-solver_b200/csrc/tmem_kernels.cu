@@ -16,27 +16,37 @@
 // rows in lockstep: every stage is full and every offset below is the same
 // for both halves.
 //
-// Per CTA (one per SM): warps 0..3 compute, warps 4..7 feed them.
-//  * Producer warp 4 + c fills consumer c's ring of ST stages.  A stage is 12
-//    TMA tiles (6 arrays x 2 halves) of R rows x 16 lines on one mbarrier;
-//    the lower half's tiles come from the mirrored arrays.  The consumer
-//    copies a stage into registers and releases the slot at once.
-//  * Factors in Tensor Memory (consumer c uses TMEM lanes 32c..32c+31, the
-//    lane quarter its warp can reach), one tcgen05.st per stage on the way
-//    down and one tcgen05.ld per stage on the way back:
+// Per CTA (one per SM), for each TMEM lane quarter c (0..3) three warps:
+// warp c eliminates (forward sweep), warp 4 + c feeds it, warp 8 + c
+// substitutes back.  The forward sweep of a tile overlaps the back
+// substitution of the previous one, so the load ring keeps draining while
+// results are written.
+//  * The feeding warp fills its ring of ST stages.  A stage is 12 TMA tiles
+//    (6 arrays x 2 halves) of R rows x 16 lines on one mbarrier; the lower
+//    half's tiles come from the mirrored arrays.  The eliminating warp copies
+//    a stage into registers and releases the slot at once.
+//  * Factors in Tensor Memory (lanes 32c..32c+31, the quarter these warps can
+//    reach), one tcgen05.st per stage on the way down and one tcgen05.ld per
+//    stage on the way back:
 //      - du2 and dw2 (W2S = false): 4 columns per FP64 row, 2 per FP32 row;
 //        512 columns hold m <= 128 (FP64) / 256 (FP32) rows, n <= 256 / 512;
 //      - du2 only (W2S = true): half the columns, n <= 512 / 1024, with dw2
 //        travelling with x2 through the caller's buffer.
+//    Consecutive tiles of a warp fill TMEM blocks in opposite orders, so the
+//    blocks the back substitution of tile t frees first are the ones the
+//    forward sweep of tile t + 1 fills first; a progress word in shared
+//    memory (tile, steps done) tells the eliminating warp when a block is
+//    free.  The carries of the two halves are handed over in shared memory
+//    behind an mbarrier.
 //  * x2 (and dw2 when W2S) make an L2 round trip through the caller's buffer
 //    ([tile][half][m][16] of x2 or (dw2, x2) pairs), written once per row and
 //    read back, most recent first, by two bulk copies per stage into a small
 //    ring; each 128-byte line is dropped from L2 (discard.global.L2) once read,
 //    so it never reaches HBM.
 //  * Output: strided directions store x directly (16 consecutive lines are one
-//    128-byte segment).  Along x, a lane's rows are contiguous in memory: the R
-//    results per half go into a 64-byte-swizzled shared tile (the layout of the
-//    loads) and leave as TMA tile stores.
+//    128-byte segment).  Along x, a lane's rows are contiguous in memory: the
+//    results of two steps go into a 128-byte-swizzled shared tile of 2R rows
+//    per half and leave as one TMA tile store (128-byte rows).
 //
 // Grids are described by jobs (tensor maps, x, buffer region, geometry).  A
 // single-grid launch passes its job as a kernel parameter; a batched launch
@@ -44,15 +54,18 @@
 // of all its grids, so one launch -- and one CUDA-graph node -- solves them all.
 //
 // Tensor views: along x {n, n_sys} with tiles {R, 16} (64-byte rows, 64-byte
-// swizzle); strided {inner, n, outer} with tiles {16, R, 1}.  TMA needs
+// swizzle; 256-byte L2 promotion, so a line's next rows are already in L2)
+// and, for the stores, {2R, 16} (128-byte swizzle); strided {inner, n, outer}
+// with tiles {16, R, 1}.  TMA needs
 // 16-byte aligned bases and row strides and 16-byte aligned innermost
 // coordinates: n * sizeof(F) % 16 == 0 along x (every row coordinate used is
 // a multiple of R), inner * sizeof(F) % 16 == 0 for the strided views.
 //
 // Waits are bounded (tma_device.cuh).  A wait that runs out raises
-// STATUS_TIMEOUT_BIT; the consumer stops its producer, drains the copies in
-// flight into its buffers (again bounded) and the CTA frees its TMEM before
-// returning.  A zero or non-finite pivot turns the carries into NaN or
+// STATUS_TIMEOUT_BIT; the warp raises its quarter's stop flag (the feeding
+// warp then issues nothing more, the other warps leave at their next wait),
+// drains the copies it has in flight (again bounded) and the CTA frees its
+// TMEM before returning.  A zero or non-finite pivot turns the carries into NaN or
 // infinity, which is checked once per tile (STATUS_ZERO_PIVOT_BIT).
 #include <algorithm>
 #include <cstdlib>
@@ -68,7 +81,7 @@ namespace penta {
 // One grid of a launch.  Layout shared by host and device; 64-byte aligned
 // for the tensor maps.
 template <typename F> struct alignas(64) TmemJob {
-  CUtensorMap maps[6];  // ds, dl, d, du, dw, x (when tma)
+  CUtensorMap maps[7];  // ds, dl, d, du, dw, x; x again with 2R-row boxes (along x)
   const F *arr[6];      // the same arrays
   F *x;
   F *scratch;           // this grid's region of the caller's buffer
@@ -96,15 +109,18 @@ template <typename F, bool CONTIG, bool W2S, int ST, int XST> struct TmemGeom {
   static constexpr int BOX = R * TS;                  // elements per TMA tile
   static constexpr int SE = 12 * BOX;                 // forward stage
   static constexpr int XE = 2 * R * TS * PW;          // read-back stage
-  static constexpr int OBE = CONTIG ? 4 * BOX : 0;    // output tiles: 2 buffers x 2 halves
+  static constexpr int OBE = CONTIG ? 8 * BOX : 0;    // output: 2 buffers x 2 halves x 2R rows
+  static constexpr int HE = 2 * 6 * 32;               // carries: 2 slots x 6 values x 32 lanes
   static constexpr int kCols = tmem_cols_per_stage<F, W2S>();
-  static constexpr size_t kData = (size_t)(ST * SE + XST * XE + OBE) * sizeof(F);
-  static constexpr size_t kBars = (size_t)(2 * ST + XST) * 8;
+  static constexpr int NB = (int)kTmemCols / kCols;   // TMEM blocks of one stage each
+  static constexpr size_t kData = (size_t)(ST * SE + XST * XE + OBE + HE) * sizeof(F);
+  static constexpr size_t kBars = (size_t)(2 * ST + XST + 2) * 8;
   static constexpr size_t kCons = (kData + kBars + 1023) / 1024 * 1024;
-  static constexpr size_t kTail = 64;                 // TMEM address + stop flags
+  static constexpr size_t kTail = 64;                 // TMEM address, stop flags, progress
   static constexpr size_t kUsed = NCONS * kCons + kTail + 1024;  // + alignment slack
   // at least 116 KB, so that one CTA holds an SM (and all of its TMEM)
   static constexpr size_t kSmem = kUsed > 118784 ? kUsed : 118784;
+  static_assert(kSmem <= 232448, "shared memory per CTA");
   static_assert(R * (W2S ? 1 : 2) * (int)sizeof(F) / 4 == kCols, "TMEM columns per stage");
 };
 
@@ -125,12 +141,12 @@ template <> __device__ __forceinline__ float get_bits<float>(const uint32_t *tv,
 }
 
 template <typename F, bool CONTIG, bool W2S, int ST, int XST, bool BATCH>
-__global__ void __launch_bounds__(64 * NCONS, 1)
+__global__ void __launch_bounds__(96 * NCONS, 1)
 tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__restrict__ jobs,
                    int n_jobs, int total_tiles, int flags, int *__restrict__ status_word) {
   using G = TmemGeom<F, CONTIG, W2S, ST, XST>;
   using V2 = typename Vec2<F>::T;
-  constexpr int R = G::R, BOX = G::BOX, SE = G::SE, XE = G::XE, PW = G::PW;
+  constexpr int R = G::R, BOX = G::BOX, SE = G::SE, XE = G::XE, PW = G::PW, NB = G::NB;
   constexpr int EPC = 16 / (int)sizeof(F);  // elements per 16-byte chunk
   constexpr int CW = (int)sizeof(F) / 4;    // TMEM columns per value
   constexpr int kMirror[6] = {4, 3, 2, 1, 0, 5};
@@ -141,16 +157,20 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
       smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   const int warp = threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
-  const int cons = warp % NCONS;  // the consumer this warp is, or feeds
+  const int role = warp / NCONS;  // 0 eliminates, 1 feeds, 2 substitutes back
+  const int cons = warp % NCONS;  // the lane quarter (and ring) this warp works on
   auto region = [&](int c) { return base + c * G::kCons; };
   F *const ring = reinterpret_cast<F *>(region(cons));
   F *const xr = ring + ST * SE;    // read-back stages [XST][2 halves][R][16][PW]
-  F *const obuf = xr + XST * XE;   // along x: [2 buffers][2 halves][BOX]
+  F *const obuf = xr + XST * XE;   // along x: [2 buffers][2 halves][2R rows x 16 lines]
+  F *const hand = obuf + G::OBE;   // carries handed over: [2 slots][6][32 lanes]
   uint64_t *const full = reinterpret_cast<uint64_t *>(region(cons) + G::kData);
   uint64_t *const empty = full + ST;
   uint64_t *const rfull = empty + ST;
+  uint64_t *const hfull = rfull + XST;  // [2]: a tile's forward sweep is done
   uint32_t *const tmem_slot = reinterpret_cast<uint32_t *>(base + NCONS * G::kCons);
   volatile int *const stop = reinterpret_cast<volatile int *>(tmem_slot + 4);  // [NCONS]
+  int *const prog = reinterpret_cast<int *>(tmem_slot + 8);                    // [NCONS]
 
   const int gw = blockIdx.x * NCONS + cons;
   const int tw = gridDim.x * NCONS;
@@ -159,8 +179,9 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   if (threadIdx.x == 0) {
     for (int c = 0; c < NCONS; ++c) {
       uint64_t *f = reinterpret_cast<uint64_t *>(region(c) + G::kData);
-      for (int s = 0; s < 2 * ST + XST; ++s) mbar_init(&f[s], s < ST ? 32 : 1);
+      for (int s = 0; s < 2 * ST + XST + 2; ++s) mbar_init(&f[s], s < ST ? 32 : 1);
       stop[c] = 0;
+      prog[c] = 0;
     }
     mbar_init_fence();
   }
@@ -183,7 +204,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   struct Geo {
     const TmemJob<F> *J;
     F *x, *scratch;
-    int n, mt, inner, tpr, n_sys, tile_base, tma;
+    int n, mt, inner, tpr, n_sys, tile_base, n_tiles, tma;
   };
   auto load_geo = [&](const TmemJob<F> *J, Geo &g) {
     g.J = J;
@@ -195,6 +216,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
     g.tpr = J->tpr;
     g.n_sys = J->n_sys;
     g.tile_base = J->tile_base;
+    g.n_tiles = J->n_tiles;
     g.tma = J->tma;
   };
   auto tile_coords = [&](const Geo &g, int tile, int &c0, int &c2) {
@@ -210,7 +232,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   // ================================ producer ================================
   // The whole warp: lane 0 issues TMA tiles (arriving for all 32 lanes), or
   // all lanes copy elements of a misaligned grid.  full[] counts 32 arrivals.
-  if (warp >= NCONS) {
+  if (role == 1) {
     int slot = 0, use = 0, cursor = 0, fenced = -1;
     Geo JG;
     load_geo(job_of(gw, cursor), JG);
@@ -311,268 +333,396 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
     return;
   }
 
-  // ================================ consumer ================================
   const int sys = lane % TS;
   const int part = lane / TS;
   const uint32_t taddr = tmem_base + ((uint32_t)(cons * 32) << 16);
-  // element offsets, inside a stage, of this lane's r-th row in elimination
-  // order (ld) and, inside an output buffer, in back-substitution order (st)
-  int ld[R], st[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int rl = part ? (R - 1 - r) : r;
-    const int rs = part ? r : (R - 1 - r);
-    if (CONTIG) {
-      const int sw = (sys >> 1) & 3;  // 64-byte swizzle: 16-byte chunk ^= (row / 2) % 4
-      ld[r] = part * BOX + sys * R + ((rl / EPC) ^ sw) * EPC + rl % EPC;
-      st[r] = part * BOX + sys * R + ((rs / EPC) ^ sw) * EPC + rs % EPC;
-    } else {
-      ld[r] = part * BOX + rl * TS + sys;
-      st[r] = 0;
-    }
-  }
-  const bool drop = (flags & 1) != 0;
 
-  int slot = 0, r_slot = 0, o_buf = 0, cursor = 0;
-  unsigned phase = 0, r_phase = 0;
-  Geo JG;
-  load_geo(job_of(gw, cursor), JG);
-  long long r_issued = 0, r_consumed = 0;
-  bool bad = false, timed_out = false;
-
-  for (int ti = 0; ti < my_tiles && !timed_out; ++ti) {
-    const int t = gw + ti * tw;
-    const TmemJob<F> *J = job_of(t, cursor);
-    if (J != JG.J) load_geo(J, JG);
-    const int tile = t - JG.tile_base;
-    int c0, c2;
-    tile_coords(JG, tile, c0, c2);
-    const int n = JG.n, mt = JG.mt, inner = JG.inner;
-    const int n_stages = mt / R;
-    const int nvp = part ? 2 * mt - n : 0;  // this half's virtual rows
-    const int count = CONTIG ? min(TS, JG.n_sys - c0) : min(TS, inner - c0);
-    const bool active = sys < count;
-    F *const x2t = JG.scratch + (long long)tile * 2 * mt * TS * PW;  // [2][m][16][PW]
-    F *const x2w = x2t + (part * mt * TS + sys) * PW;                // row k at + k * 16 PW
-
-    // ------------------------------ forward ---------------------------------
-    Carry<F> c;
-    c.zero();
-    for (int g = 0; g < n_stages; ++g) {
-      if (!__all_sync(0xffffffffu, mbar_wait(&full[slot], phase))) {
-        timed_out = true;
-        break;
-      }
-      const F *v = ring + slot * SE;
-      F a[R][6];
+  if (role == 0) {
+    // ============================ forward sweep ==============================
+    // Tile ti stores stage g's factors in TMEM block g (even ti) or NB-1-g
+    // (odd ti).  The back-substitution of the previous tile reads its blocks
+    // in the order that frees exactly the ones this tile fills first, and
+    // publishes its progress in prog[cons] = tile * 65536 + steps done: block
+    // b of this tile is free once that tile has done b's share of its steps.
+    int ld[R];  // element offset, inside a stage, of this lane's r-th row
 #pragma unroll
-      for (int r = 0; r < R; ++r)
-#pragma unroll
-        for (int q = 0; q < 6; ++q) a[r][q] = v[ld[r] + q * 2 * BOX];
-      if (g * R < nvp + 2) {  // virtual rows, and couplings that leave the line
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int k = g * R + r;
-          if (k < nvp) {
-#pragma unroll
-            for (int q = 0; q < 6; ++q) a[r][q] = (q == 2) ? F(1) : F(0);
-          }
-          if (k == nvp || k == nvp + 1) a[r][0] = F(0);
-          if (k == nvp) a[r][1] = F(0);
-        }
-      }
-      fence_async_shared();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[slot]);
-      if (++slot == ST) {
-        slot = 0;
-        phase ^= 1u;
-      }
-      F u[R], w[R], y[R];
-#pragma unroll
-      for (int r = 0; r < R; ++r)
-        fwd_row_lean(a[r][0], a[r][1], a[r][2], a[r][3], a[r][4], a[r][5], c, u[r], w[r],
-                     y[r]);
-      uint32_t tv[G::kCols];
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        put_bits<F>(tv, r * CW * (W2S ? 1 : 2), u[r]);
-        if (!W2S) put_bits<F>(tv, r * CW * 2 + CW, w[r]);
-      }
-      if constexpr (G::kCols == 32)
-        tmem_store32(taddr + (uint32_t)(g * G::kCols), reinterpret_cast<uint32_t(&)[32]>(tv));
-      else
-        tmem_store16(taddr + (uint32_t)(g * G::kCols), reinterpret_cast<uint32_t(&)[16]>(tv));
-      F *const x2g = x2w + g * R * TS * PW;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        if constexpr (W2S) {
-          V2 pv;
-          pv.x = w[r];
-          pv.y = y[r];
-          *reinterpret_cast<V2 *>(x2g + r * TS * 2) = pv;
-        } else {
-          x2g[r * TS] = y[r];
-        }
+    for (int r = 0; r < R; ++r) {
+      const int rl = part ? (R - 1 - r) : r;
+      if (CONTIG) {
+        const int sw = (sys >> 1) & 3;  // 64-byte swizzle: 16-byte chunk ^= (row / 2) % 4
+        ld[r] = part * BOX + sys * R + ((rl / EPC) ^ sw) * EPC + rl % EPC;
+      } else {
+        ld[r] = part * BOX + rl * TS + sys;
       }
     }
-    if (timed_out) break;
-    if (active)
-      bad |= !(isfinite(c.u1) && isfinite(c.u2) && isfinite(c.w1) && isfinite(c.w2) &&
-               isfinite(c.y1) && isfinite(c.y2));
-    // the read-back copies (async proxy) read what this warp has just stored
-    fence_async_global();
-    __syncwarp();
-
-    // ------------------------------ interface -------------------------------
-    const F pu1 = __shfl_xor_sync(0xffffffffu, c.u1, TS);
-    const F pu2 = __shfl_xor_sync(0xffffffffu, c.u2, TS);
-    const F pw1 = __shfl_xor_sync(0xffffffffu, c.w1, TS);
-    const F pw2 = __shfl_xor_sync(0xffffffffu, c.w2, TS);
-    const F py1 = __shfl_xor_sync(0xffffffffu, c.y1, TS);
-    const F py2 = __shfl_xor_sync(0xffffffffu, c.y2, TS);
-    F u0, u1, u2, u3;
-    if (part == 0)
-      solve_interface(c.u2, c.w2, c.y2, c.u1, c.w1, c.y1, pu1, pw1, py1, pu2, pw2, py2, u0,
-                      u1, u2, u3);
-    else
-      solve_interface(pu2, pw2, py2, pu1, pw1, py1, c.u1, c.w1, c.y1, c.u2, c.w2, c.y2, u0,
-                      u1, u2, u3);
-    F xa = part ? u1 : u2;  // x of the row just past this half's last row
-    F xb = part ? u0 : u3;  // and of the one after it
-
-    // ------------------------------ backward --------------------------------
-    // stage s: elimination rows k in [m - (s+1) R, m - s R) of both halves
-    constexpr unsigned kBlock = (unsigned)(R * TS * PW * sizeof(F));  // one half, one stage
-    int ri_slot = r_slot;
-    auto rissue = [&](int s) {
-      if (s >= n_stages) return;
-      if (lane == 0) {
-        const int k0 = mt - (s + 1) * R;
-        F *dst = xr + ri_slot * XE;
-        mbar_expect_tx(&rfull[ri_slot], 2u * kBlock);
-        bulk_load(dst, x2t + (long long)k0 * TS * PW, kBlock, &rfull[ri_slot]);
-        bulk_load(dst + R * TS * PW, x2t + (long long)(mt + k0) * TS * PW, kBlock,
-                  &rfull[ri_slot]);
-      }
-      ++r_issued;
-      if (++ri_slot == XST) ri_slot = 0;
-    };
-    for (int s = 0; s < XST; ++s) rissue(s);
-
-    for (int s = 0; s < n_stages; ++s) {
-      if (!__all_sync(0xffffffffu, mbar_wait(&rfull[r_slot], r_phase))) {
-        timed_out = true;
-        break;
-      }
-      const F *xsrc = xr + r_slot * XE + (part * R * TS + sys) * PW;
-      F xs[R], du[R], dw[R];
-      uint32_t tv[G::kCols];
-      if constexpr (G::kCols == 32)
-        tmem_load32(taddr + (uint32_t)((n_stages - 1 - s) * G::kCols),
-                    reinterpret_cast<uint32_t(&)[32]>(tv));
-      else
-        tmem_load16(taddr + (uint32_t)((n_stages - 1 - s) * G::kCols),
-                    reinterpret_cast<uint32_t(&)[16]>(tv));
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const int j = R - 1 - r;  // row inside the stage block
-        if constexpr (W2S) {
-          const V2 pv = *reinterpret_cast<const V2 *>(xsrc + j * TS * 2);
-          dw[r] = pv.x;
-          xs[r] = pv.y;
-          du[r] = get_bits<F>(tv, j * CW);
-        } else {
-          xs[r] = xsrc[j * TS];
-          du[r] = get_bits<F>(tv, j * CW * 2);
-          dw[r] = get_bits<F>(tv, j * CW * 2 + CW);
+    int slot = 0, cursor = 0, n_prev = 0, seen = 0;
+    unsigned phase = 0;
+    Geo JG;
+    load_geo(job_of(gw, cursor), JG);
+    bool bad = false;
+    int fail = 0;  // 0 fine, 1 a wait ran out, 2 stopped by another warp
+    int ti = 0;
+    for (; ti < my_tiles; ++ti) {
+      const int t = gw + ti * tw;
+      const TmemJob<F> *J = job_of(t, cursor);
+      if (J != JG.J) load_geo(J, JG);
+      const int tile = t - JG.tile_base;
+      int c0, c2;
+      tile_coords(JG, tile, c0, c2);
+      const int n = JG.n, mt = JG.mt;
+      const int n_stages = mt / R;
+      const int nvp = part ? 2 * mt - n : 0;  // this half's virtual rows
+      const int count = CONTIG ? min(TS, JG.n_sys - c0) : min(TS, JG.inner - c0);
+      F *const x2w = JG.scratch + (long long)tile * 2 * mt * TS * PW + (part * mt * TS + sys) * PW;
+      const bool flip = (ti & 1) != 0;
+      const int free_blocks = NB - n_prev;  // blocks the previous tile never used
+      Carry<F> c;
+      c.zero();
+      for (int g = 0; g < n_stages; ++g) {
+        if (!__all_sync(0xffffffffu, mbar_wait(&full[slot], phase))) {
+          fail = 1;
+          break;
         }
-      }
-      if (CONTIG && lane == 0) bulk_wait_read<1>();  // output buffer o_buf is free
-      fence_async_shared();
-      __syncwarp();
-      ++r_consumed;
-      rissue(s + XST);  // refills the slot just read (ri_slot == r_slot here)
-      if (++r_slot == XST) {
-        r_slot = 0;
-        r_phase ^= 1u;
-      }
-      // the stage's block of each half is dead: drop its 128-byte lines
-      constexpr int kLines = (int)(kBlock / 128);
-      if (drop && sys < kLines)
-        discard_l2_line(reinterpret_cast<const unsigned char *>(
-                            x2t + (long long)(part * mt + mt - (s + 1) * R) * TS * PW) +
-                        sys * 128);
-      F xk[R];
+        const F *v = ring + slot * SE;
+        F a[R][6];
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        xk[r] = xs[r] - dw[r] * xb - du[r] * xa;
-        xb = xa;
-        xa = xk[r];
-      }
-      if (CONTIG && !JG.tma) {  // misaligned grid: each lane writes its own rows
-        if (active) {
-          F *const p = JG.x + (long long)(c0 + sys) * n;
-          const int row0 = part ? (mt + s * R) : (mt - 1 - s * R);
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+          for (int q = 0; q < 6; ++q) a[r][q] = v[ld[r] + q * 2 * BOX];
+        if (g * R < nvp + 2) {  // virtual rows, and couplings that leave the line
 #pragma unroll
           for (int r = 0; r < R; ++r) {
-            const int row = part ? row0 + r : row0 - r;
-            if (row < n) p[row] = xk[r];
+            const int k = g * R + r;
+            if (k < nvp) {
+#pragma unroll
+              for (int q = 0; q < 6; ++q) a[r][q] = (q == 2) ? F(1) : F(0);
+            }
+            if (k == nvp || k == nvp + 1) a[r][0] = F(0);
+            if (k == nvp) a[r][1] = F(0);
           }
         }
-      } else if (CONTIG) {
-        F *const ob = obuf + o_buf * 2 * BOX;
-#pragma unroll
-        for (int r = 0; r < R; ++r) ob[st[r]] = xk[r];
         fence_async_shared();
         __syncwarp();
-        if (lane == 0) {
-          tma_store_2d(&J->maps[5], ob, mt - (s + 1) * R, c0);
-          if (mt + s * R < n) tma_store_2d(&J->maps[5], ob + BOX, mt + s * R, c0);
-          bulk_commit();
+        if (lane == 0) mbar_arrive(&empty[slot]);
+        if (++slot == ST) {
+          slot = 0;
+          phase ^= 1u;
         }
-        o_buf ^= 1;
-      } else if (active) {
-        // the upper half runs towards row 0, the lower half towards row n - 1
-        const int row0 = part ? (mt + s * R) : (mt - 1 - s * R);
-        const long long step = part ? (long long)inner : -(long long)inner;
-        F *const p = JG.x + (long long)c2 * inner * n + c0 + sys + (long long)row0 * inner;
-        if (part == 0 || mt + (s + 1) * R <= n) {
+        F u[R], w[R], y[R];
 #pragma unroll
-          for (int r = 0; r < R; ++r) p[r * step] = xk[r];
-        } else {  // the lower half's last stages end in virtual rows
+        for (int r = 0; r < R; ++r)
+          fwd_row_lean(a[r][0], a[r][1], a[r][2], a[r][3], a[r][4], a[r][5], c, u[r], w[r],
+                       y[r]);
+        uint32_t tv[G::kCols];
 #pragma unroll
-          for (int r = 0; r < R; ++r)
-            if (row0 + r < n) p[r * step] = xk[r];
+        for (int r = 0; r < R; ++r) {
+          put_bits<F>(tv, r * CW * (W2S ? 1 : 2), u[r]);
+          if (!W2S) put_bits<F>(tv, r * CW * 2 + CW, w[r]);
+        }
+        // wait (lane 0, bounded) until the previous tile has read this block
+        const int need = (ti - 1) * 65536 + max(0, g + 1 - free_blocks);
+        int ok = 1;
+        if (lane == 0 && seen < need) {
+          seen = ld_acquire_shared(&prog[cons]);
+          if (seen < need) {
+            const unsigned long long t0 = global_ns();
+            for (;;) {
+              __nanosleep(32);
+              seen = ld_acquire_shared(&prog[cons]);
+              if (seen >= need) break;
+              if (stop[cons] != 0) {
+                ok = 2;
+                break;
+              }
+              if (global_ns() - t0 > 2000000000ull) {
+                ok = 0;
+                break;
+              }
+            }
+          }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (ok != 1) {
+          fail = ok == 0 ? 1 : 2;
+          break;
+        }
+        tmem_fence_after_sync();
+        const int blk = flip ? NB - 1 - g : g;
+        if constexpr (G::kCols == 32)
+          tmem_store32(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[32]>(tv));
+        else
+          tmem_store16(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[16]>(tv));
+        F *const x2g = x2w + g * R * TS * PW;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if constexpr (W2S) {
+            V2 pv;
+            pv.x = w[r];
+            pv.y = y[r];
+            *reinterpret_cast<V2 *>(x2g + r * TS * 2) = pv;
+          } else {
+            x2g[r * TS] = y[r];
+          }
         }
       }
+      n_prev = n_stages;
+      if (fail) break;
+      if (sys < count)
+        bad |= !(isfinite(c.u1) && isfinite(c.u2) && isfinite(c.w1) && isfinite(c.w2) &&
+                 isfinite(c.y1) && isfinite(c.y2));
+      // hand the carries to the back-substitution warp; the x2 stores above
+      // are read next by its bulk copies (async proxy)
+      F *const h = hand + (ti & 1) * 6 * 32 + lane;
+      h[0] = c.u1;
+      h[32] = c.u2;
+      h[64] = c.w1;
+      h[96] = c.w2;
+      h[128] = c.y1;
+      h[160] = c.y2;
+      fence_async_global();
+      tmem_fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&hfull[ti & 1]);
     }
+    if (fail) {
+      stop[cons] = 1;  // the producer issues nothing more
+      // wake the back-substitution warp if it waits for this tile
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&hfull[ti & 1]);
+      // drain what may still land in the ring (bounded waits)
+      for (int k = 0; k < ST; ++k) {
+        if (!mbar_wait(&full[slot], phase)) break;
+        if (++slot == ST) {
+          slot = 0;
+          phase ^= 1u;
+        }
+      }
+      if (fail == 1 && lane == 0) atomicOr(status_word, STATUS_TIMEOUT_BIT);
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status_word, STATUS_ZERO_PIVOT_BIT);
+  } else {
+    // ========================= back-substitution ============================
+    // Along x the results of two steps leave together as one tile of 2R rows
+    // (128-byte rows, 128-byte swizzle) per half; st2[r] is the offset, in a
+    // half's tile, of this lane's r-th row of an even step (an odd step's is
+    // st2[r] ^ R: its rows are the other R of the tile).  A last step without
+    // a partner uses R-row tiles (64-byte swizzle, offsets st1).
+    int st1[R], st2[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (CONTIG) {
+        const int rs = part ? r : (R - 1 - r);
+        st1[r] = part * 2 * BOX + sys * R + ((rs / EPC) ^ ((sys >> 1) & 3)) * EPC + rs % EPC;
+        const int rr = part ? r : (2 * R - 1 - r);
+        st2[r] = part * 2 * BOX + sys * 2 * R + ((rr / EPC) ^ (sys & 7)) * EPC + rr % EPC;
+      } else {
+        st1[r] = st2[r] = 0;
+      }
+    }
+    const bool drop = (flags & 1) != 0;
+    int r_slot = 0, o_buf = 0, cursor = 0;
+    unsigned r_phase = 0;
+    Geo JG;
+    load_geo(job_of(gw, cursor), JG);
+    long long r_issued = 0, r_consumed = 0;
+    int fail = 0;
+    for (int ti = 0; ti < my_tiles && !fail; ++ti) {
+      const int t = gw + ti * tw;
+      const TmemJob<F> *J = job_of(t, cursor);
+      if (J != JG.J) load_geo(J, JG);
+      const int tile = t - JG.tile_base;
+      int c0, c2;
+      tile_coords(JG, tile, c0, c2);
+      const int n = JG.n, mt = JG.mt, inner = JG.inner;
+      const int n_stages = mt / R;
+      const int count = CONTIG ? min(TS, JG.n_sys - c0) : min(TS, inner - c0);
+      const bool active = sys < count;
+      F *const x2t = JG.scratch + (long long)tile * 2 * mt * TS * PW;  // [2][m][16][PW]
+      const bool flip = (ti & 1) != 0;
+
+      // the forward sweep of this tile: factors in TMEM, x2 in the buffer
+      if (!__all_sync(0xffffffffu, mbar_wait(&hfull[ti & 1], (unsigned)(ti >> 1) & 1u))) {
+        fail = 1;
+        break;
+      }
+      if (stop[cons] != 0) {
+        fail = 2;
+        break;
+      }
+      tmem_fence_after_sync();
+
+      // read-back copies of x2 (most recent rows first)
+      constexpr unsigned kBlock = (unsigned)(R * TS * PW * sizeof(F));  // one half, one stage
+      int ri_slot = r_slot;
+      auto rissue = [&](int s) {
+        if (s >= n_stages) return;
+        if (lane == 0) {
+          const int k0 = mt - (s + 1) * R;
+          F *dst = xr + ri_slot * XE;
+          mbar_expect_tx(&rfull[ri_slot], 2u * kBlock);
+          bulk_load(dst, x2t + (long long)k0 * TS * PW, kBlock, &rfull[ri_slot]);
+          bulk_load(dst + R * TS * PW, x2t + (long long)(mt + k0) * TS * PW, kBlock,
+                    &rfull[ri_slot]);
+        }
+        ++r_issued;
+        if (++ri_slot == XST) ri_slot = 0;
+      };
+      for (int s = 0; s < XST; ++s) rissue(s);
+
+      // ---------------------------- interface -------------------------------
+      const F *const h = hand + (ti & 1) * 6 * 32 + lane;
+      Carry<F> c;
+      c.u1 = h[0];
+      c.u2 = h[32];
+      c.w1 = h[64];
+      c.w2 = h[96];
+      c.y1 = h[128];
+      c.y2 = h[160];
+      const F pu1 = __shfl_xor_sync(0xffffffffu, c.u1, TS);
+      const F pu2 = __shfl_xor_sync(0xffffffffu, c.u2, TS);
+      const F pw1 = __shfl_xor_sync(0xffffffffu, c.w1, TS);
+      const F pw2 = __shfl_xor_sync(0xffffffffu, c.w2, TS);
+      const F py1 = __shfl_xor_sync(0xffffffffu, c.y1, TS);
+      const F py2 = __shfl_xor_sync(0xffffffffu, c.y2, TS);
+      F u0, u1, u2, u3;
+      if (part == 0)
+        solve_interface(c.u2, c.w2, c.y2, c.u1, c.w1, c.y1, pu1, pw1, py1, pu2, pw2, py2, u0,
+                        u1, u2, u3);
+      else
+        solve_interface(pu2, pw2, py2, pu1, pw1, py1, c.u1, c.w1, c.y1, c.u2, c.w2, c.y2, u0,
+                        u1, u2, u3);
+      F xa = part ? u1 : u2;  // x of the row just past this half's last row
+      F xb = part ? u0 : u3;  // and of the one after it
+
+      // ---------------------------- backward --------------------------------
+      // step s: elimination rows k in [m - (s+1) R, m - s R) of both halves
+      for (int s = 0; s < n_stages; ++s) {
+        const int g = n_stages - 1 - s;  // the forward stage being undone
+        const int blk = flip ? NB - 1 - g : g;
+        uint32_t tv[G::kCols];
+        if constexpr (G::kCols == 32)
+          tmem_load32(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[32]>(tv));
+        else
+          tmem_load16(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[16]>(tv));
+        // the block is free for the next tile's forward sweep
+        tmem_fence_before_sync();
+        __syncwarp();
+        if (lane == 0) st_release_shared(&prog[cons], ti * 65536 + s + 1);
+        if (!__all_sync(0xffffffffu, mbar_wait(&rfull[r_slot], r_phase))) {
+          fail = 1;
+          break;
+        }
+        const F *xsrc = xr + r_slot * XE + (part * R * TS + sys) * PW;
+        F xs[R], du[R], dw[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int j = R - 1 - r;  // row inside the stage block
+          if constexpr (W2S) {
+            const V2 pv = *reinterpret_cast<const V2 *>(xsrc + j * TS * 2);
+            dw[r] = pv.x;
+            xs[r] = pv.y;
+            du[r] = get_bits<F>(tv, j * CW);
+          } else {
+            xs[r] = xsrc[j * TS];
+            du[r] = get_bits<F>(tv, j * CW * 2);
+            dw[r] = get_bits<F>(tv, j * CW * 2 + CW);
+          }
+        }
+        if (CONTIG && (s & 1) == 0 && lane == 0) bulk_wait_read<1>();  // buffer o_buf is free
+        fence_async_shared();
+        __syncwarp();
+        ++r_consumed;
+        rissue(s + XST);  // refills the slot just read (ri_slot == r_slot here)
+        if (++r_slot == XST) {
+          r_slot = 0;
+          r_phase ^= 1u;
+        }
+        // the stage's block of each half is dead: drop its 128-byte lines
+        constexpr int kLines = (int)(kBlock / 128);
+        if (drop && sys < kLines)
+          discard_l2_line(reinterpret_cast<const unsigned char *>(
+                              x2t + (long long)(part * mt + mt - (s + 1) * R) * TS * PW) +
+                          sys * 128);
+        F xk[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          xk[r] = xs[r] - dw[r] * xb - du[r] * xa;
+          xb = xa;
+          xa = xk[r];
+        }
+        if (CONTIG && !JG.tma) {  // misaligned grid: each lane writes its own rows
+          if (active) {
+            F *const p = JG.x + (long long)(c0 + sys) * n;
+            const int row0 = part ? (mt + s * R) : (mt - 1 - s * R);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int row = part ? row0 + r : row0 - r;
+              if (row < n) p[row] = xk[r];
+            }
+          }
+        } else if (CONTIG) {
+          F *const ob = obuf + o_buf * 4 * BOX;
+          if ((s & 1) == 0 && s + 1 == n_stages) {  // a last step without a partner
+#pragma unroll
+            for (int r = 0; r < R; ++r) ob[st1[r]] = xk[r];
+            fence_async_shared();
+            __syncwarp();
+            if (lane == 0) {
+              tma_store_2d(&J->maps[5], ob, mt - (s + 1) * R, c0);
+              if (mt + s * R < n) tma_store_2d(&J->maps[5], ob + 2 * BOX, mt + s * R, c0);
+              bulk_commit();
+            }
+          } else {
+            const int odd = (s & 1) ? R : 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r) ob[st2[r] ^ odd] = xk[r];
+            if (odd) {  // steps s - 1 and s: rows [mt - (s+1) R, mt - (s-1) R) of each half
+              fence_async_shared();
+              __syncwarp();
+              if (lane == 0) {
+                tma_store_2d(&J->maps[6], ob, mt - (s + 1) * R, c0);
+                if (mt + (s - 1) * R < n) tma_store_2d(&J->maps[6], ob + 2 * BOX, mt + (s - 1) * R, c0);
+                bulk_commit();
+              }
+              o_buf ^= 1;
+            }
+          }
+        } else if (active) {
+          // the upper half runs towards row 0, the lower half towards row n - 1
+          const int row0 = part ? (mt + s * R) : (mt - 1 - s * R);
+          const long long step = part ? (long long)inner : -(long long)inner;
+          F *const p = JG.x + (long long)c2 * inner * n + c0 + sys + (long long)row0 * inner;
+          if (part == 0 || mt + (s + 1) * R <= n) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) p[r * step] = xk[r];
+          } else {  // the lower half's last stages end in virtual rows
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+              if (row0 + r < n) p[r * step] = xk[r];
+          }
+        }
+      }
+      if (lane == 0) st_release_shared(&prog[cons], (ti + 1) * 65536);
+    }
+    if (fail) {
+      stop[cons] = 1;
+      // drain the read-back copies in flight (bounded waits)
+      for (; r_consumed < r_issued; ++r_consumed) {
+        if (!mbar_wait(&rfull[r_slot], r_phase)) break;
+        if (++r_slot == XST) {
+          r_slot = 0;
+          r_phase ^= 1u;
+        }
+      }
+      if (fail == 1 && lane == 0) atomicOr(status_word, STATUS_TIMEOUT_BIT);
+    }
+    if (CONTIG && lane == 0) bulk_wait<0>();
   }
 
-  if (timed_out) {
-    stop[cons] = 1;  // the producer issues nothing more
-    // drain what may still land in this consumer's buffers (bounded waits)
-    for (int k = 0; k < ST; ++k) {
-      if (!mbar_wait(&full[slot], phase)) break;
-      if (++slot == ST) {
-        slot = 0;
-        phase ^= 1u;
-      }
-    }
-    for (; r_consumed < r_issued; ++r_consumed) {
-      if (!mbar_wait(&rfull[r_slot], r_phase)) break;
-      if (++r_slot == XST) {
-        r_slot = 0;
-        r_phase ^= 1u;
-      }
-    }
-    if (lane == 0) atomicOr(status_word, STATUS_TIMEOUT_BIT);
-  }
-  if (CONTIG && lane == 0) bulk_wait<0>();
-  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status_word, STATUS_ZERO_PIVOT_BIT);
-  // all consumers are done with Tensor Memory: warp 0 frees it
+  // the forward and back-substitution warps are done with Tensor Memory:
+  // warp 0 frees it
   tmem_fence_before_sync();
-  asm volatile("bar.sync 1, %0;\n" ::"n"(32 * NCONS) : "memory");
+  asm volatile("bar.sync 1, %0;\n" ::"n"(64 * NCONS) : "memory");
   tmem_fence_after_sync();
   if (warp == 0) tmem_dealloc(tmem_base, kTmemCols);
 }
@@ -581,7 +731,8 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
 // Host side
 // ---------------------------------------------------------------------------
 template <typename F>
-bool encode(CUtensorMap *m, const F *ptr, const Lines &L, bool contig, int R) {
+bool encode(CUtensorMap *m, const F *ptr, const Lines &L, bool contig, int R,
+            bool wide = false) {
   auto fn = tensor_map_encoder();
   if (fn == nullptr) return false;
   const CUtensorMapDataType dt =
@@ -590,11 +741,12 @@ bool encode(CUtensorMap *m, const F *ptr, const Lines &L, bool contig, int R) {
   if (contig) {
     const cuuint64_t dims[2] = {(cuuint64_t)L.n, (cuuint64_t)L.n_sys};
     const cuuint64_t strides[1] = {(cuuint64_t)L.n * sizeof(F)};
-    const cuuint32_t box[2] = {(cuuint32_t)R, (cuuint32_t)TS};
+    const cuuint32_t box[2] = {(cuuint32_t)(wide ? 2 * R : R), (cuuint32_t)TS};
     const cuuint32_t es[2] = {1, 1};
     r = fn(m, dt, 2, const_cast<F *>(ptr), dims, strides, box, es,
-           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
-           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+           CU_TENSOR_MAP_INTERLEAVE_NONE,
+           wide ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   } else {
     const cuuint64_t dims[3] = {(cuuint64_t)L.inner, (cuuint64_t)L.n,
                                 (cuuint64_t)(L.n_sys / L.inner)};
@@ -661,6 +813,7 @@ bool fill_job(TmemJob<F> &J, const SolveArgs<F> &a, bool contig, F *scratch, int
     J.arr[q] = ptrs[q];
     if (J.tma && !encode<F>(&J.maps[q], ptrs[q], a.L, contig, R)) J.tma = 0;
   }
+  if (J.tma && contig && !encode<F>(&J.maps[6], a.x, a.L, contig, R, true)) J.tma = 0;
   J.x = a.x;
   J.scratch = scratch;
   J.n = (int)a.L.n;
@@ -685,7 +838,7 @@ cudaError_t tmem_launch_raw(const TmemJob<F> &job1, const TmemJob<F> *jobs, int 
   const int need = (total_tiles + NCONS - 1) / NCONS;
   const int grid = need < sm_count ? need : sm_count;
   if (grid <= 0) return cudaSuccess;
-  kern<<<grid, 64 * NCONS, G::kSmem, stream>>>(job1, jobs, n_jobs, total_tiles, flags, status);
+  kern<<<grid, 96 * NCONS, G::kSmem, stream>>>(job1, jobs, n_jobs, total_tiles, flags, status);
   return cudaGetLastError();
 }
 
@@ -695,7 +848,7 @@ template <typename F, bool CONTIG, bool W2S, int ST, int XST> int tmem_occ() {
   int blocks = 0;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)G::kSmem) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, 64 * NCONS, G::kSmem) !=
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, 96 * NCONS, G::kSmem) !=
           cudaSuccess) {
     cudaGetLastError();
     return 0;
@@ -712,13 +865,15 @@ template <typename F, bool CONTIG, bool W2S, int ST, int XST> int tmem_occ() {
   X(double, true, false, 3, 4)  \
   X(double, true, false, 3, 3)  \
   X(double, false, false, 3, 4) \
-  X(double, false, false, 4, 3) \
-  X(double, true, true, 3, 3)   \
+  X(double, false, false, 3, 3) \
+  X(double, false, false, 4, 2) \
+  X(double, false, false, 4, 1) \
+  X(double, true, true, 3, 2)   \
   X(double, false, true, 3, 4)  \
   X(float, true, false, 3, 4)   \
   X(float, false, false, 3, 4)  \
   X(float, false, false, 4, 3)  \
-  X(float, true, true, 3, 3)    \
+  X(float, true, true, 3, 2)    \
   X(float, false, true, 3, 4)
 
 template <typename F> const std::vector<TmemConfig> &tmem_configs() {
@@ -771,7 +926,7 @@ cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count
   TmemJob<F> J;
   if (!fill_job<F>(J, a, c.contig, static_cast<F *>(a.scratch), 0))
     return cudaErrorInvalidValue;
-  const int flags = (reinterpret_cast<uintptr_t>(a.scratch) % 128 == 0) ? 1 : 0;
+  const int flags = ((reinterpret_cast<uintptr_t>(a.scratch) % 128 == 0) ? 1 : 0);
 #define PENTA_X(FT_, C_, W_, ST_, XST_)                                                   \
   if (std::is_same<F, FT_>::value && c.contig == C_ && c.w2s == W_ && c.stages == ST_ &&  \
       c.xstages == XST_)                                                                  \
@@ -814,7 +969,7 @@ cudaError_t launch_tmem_batch(const void *device_jobs, int n_jobs, int total_til
     return tmem_launch_raw<F, true, false, 3, 4, true>(none, jobs, n_jobs, total_tiles, flags,
                                                        sm_count, status, stream);
   if (contig && w2s)
-    return tmem_launch_raw<F, true, true, 3, 3, true>(none, jobs, n_jobs, total_tiles, flags,
+    return tmem_launch_raw<F, true, true, 3, 2, true>(none, jobs, n_jobs, total_tiles, flags,
                                                       sm_count, status, stream);
   if (!w2s)
     return tmem_launch_raw<F, false, false, 3, 4, true>(none, jobs, n_jobs, total_tiles, flags,
