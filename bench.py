@@ -167,11 +167,11 @@ def run_ours(args):
     def step(x, dir_events=None):
         for it in range(ITERS):
             for axis in range(3):
-                if dir_events is not None and it == 0:
-                    dir_events[axis][0].record(stream)
+                if dir_events is not None:
+                    dir_events[it][axis][0].record(stream)
                 solve(axis, x)
-                if dir_events is not None and it == 0:
-                    dir_events[axis][1].record(stream)
+                if dir_events is not None:
+                    dir_events[it][axis][1].record(stream)
 
     x = d["x"]
     torch.cuda.synchronize()
@@ -185,8 +185,10 @@ def run_ours(args):
     # ---- timed region: K steps, device time ---------------------------------
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    dir_ev = [[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(3)]
-              for _ in range(args.steps)]
+    # an event pair around every launch of the timed region (average launch
+    # duration per direction, for the roofline)
+    dir_ev = [[[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(3)]
+               for _ in range(ITERS)] for _ in range(args.steps)]
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -204,8 +206,9 @@ def run_ours(args):
         ms_total = float(t.item())
         dist.barrier()
     ms_step = ms_total / args.steps
-    per_dir_ms = [statistics.mean(dir_ev[k][a][0].elapsed_time(dir_ev[k][a][1])
-                                  for k in range(args.steps)) for a in range(3)]
+    per_dir_ms = [statistics.mean(dir_ev[k][it][a][0].elapsed_time(dir_ev[k][it][a][1])
+                                  for k in range(args.steps) for it in range(ITERS))
+                  for a in range(3)]
     alg_bytes_step = BYTES_PER_POINT_AXIS * n ** 3 * 3 * ITERS
     value = world * alg_bytes_step / (ms_step * 1e-3) / 1e9
 

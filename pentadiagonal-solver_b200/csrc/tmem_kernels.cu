@@ -42,7 +42,10 @@
 //    ([tile][half][m][16] of x2 or (dw2, x2) pairs), written once per row and
 //    read back, most recent first, by two bulk copies per stage into a small
 //    ring; each 128-byte line is dropped from L2 (discard.global.L2) once read,
-//    so it never reaches HBM.
+//    so it never reaches HBM.  The stores carry an evict-last L2 policy and
+//    the streamed accesses (coefficient and right-hand-side loads -- along x
+//    with dw2 in the buffer excepted --, results, read-backs) an evict-first
+//    one, so that the scratch survives in L2 while the arrays stream past it.
 //  * Output: strided directions store x directly (16 consecutive lines are one
 //    128-byte segment).  Along x, a lane's rows are contiguous in memory: the
 //    results of two steps go into a 128-byte-swizzled shared tile of 2R rows
@@ -233,6 +236,9 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   // The whole warp: lane 0 issues TMA tiles (arriving for all 32 lanes), or
   // all lanes copy elements of a misaligned grid.  full[] counts 32 arrivals.
   if (role == 1) {
+    // read once: evict first -- except along x with dw2 in the buffer, where
+    // the larger scratch round trip does better against normal-priority loads
+    const uint64_t pol_in = (CONTIG && W2S) ? l2_policy_normal() : l2_policy_first();
     int slot = 0, use = 0, cursor = 0, fenced = -1;
     Geo JG;
     load_geo(job_of(gw, cursor), JG);
@@ -280,15 +286,16 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
 #pragma unroll
             for (int q = 0; q < 6; ++q) {
               if (CONTIG) {
-                tma_load_2d(dst + (2 * q) * BOX, &J->maps[q], &full[slot], r_up, c0);
+                tma_load_2d_hint(dst + (2 * q) * BOX, &J->maps[q], &full[slot], r_up, c0, pol_in);
                 if (lower)
-                  tma_load_2d(dst + (2 * q + 1) * BOX, &J->maps[kMirror[q]], &full[slot],
-                              r_dn, c0);
+                  tma_load_2d_hint(dst + (2 * q + 1) * BOX, &J->maps[kMirror[q]], &full[slot],
+                                   r_dn, c0, pol_in);
               } else {
-                tma_load_3d(dst + (2 * q) * BOX, &J->maps[q], &full[slot], c0, r_up, c2);
+                tma_load_3d_hint(dst + (2 * q) * BOX, &J->maps[q], &full[slot], c0, r_up, c2,
+                                 pol_in);
                 if (lower)
-                  tma_load_3d(dst + (2 * q + 1) * BOX, &J->maps[kMirror[q]], &full[slot], c0,
-                              r_dn, c2);
+                  tma_load_3d_hint(dst + (2 * q + 1) * BOX, &J->maps[kMirror[q]], &full[slot],
+                                   c0, r_dn, c2, pol_in);
               }
             }
           }
@@ -355,6 +362,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         ld[r] = part * BOX + rl * TS + sys;
       }
     }
+    const uint64_t pol_x2 = l2_policy_last();  // read back soon: keep in L2
     int slot = 0, cursor = 0, n_prev = 0, seen = 0;
     unsigned phase = 0;
     Geo JG;
@@ -459,9 +467,9 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
             V2 pv;
             pv.x = w[r];
             pv.y = y[r];
-            *reinterpret_cast<V2 *>(x2g + r * TS * 2) = pv;
+            st_hint(reinterpret_cast<V2 *>(x2g + r * TS * 2), pv, pol_x2);
           } else {
-            x2g[r * TS] = y[r];
+            st_hint(x2g + r * TS, y[r], pol_x2);
           }
         }
       }
@@ -520,6 +528,8 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
       }
     }
     const bool drop = (flags & 1) != 0;
+    const uint64_t pol_out = l2_policy_first();  // written once
+    const uint64_t pol_rb = l2_policy_first();   // read once (then dropped)
     int r_slot = 0, o_buf = 0, cursor = 0;
     unsigned r_phase = 0;
     Geo JG;
@@ -560,9 +570,9 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
           const int k0 = mt - (s + 1) * R;
           F *dst = xr + ri_slot * XE;
           mbar_expect_tx(&rfull[ri_slot], 2u * kBlock);
-          bulk_load(dst, x2t + (long long)k0 * TS * PW, kBlock, &rfull[ri_slot]);
-          bulk_load(dst + R * TS * PW, x2t + (long long)(mt + k0) * TS * PW, kBlock,
-                    &rfull[ri_slot]);
+          bulk_load_hint(dst, x2t + (long long)k0 * TS * PW, kBlock, &rfull[ri_slot], pol_rb);
+          bulk_load_hint(dst + R * TS * PW, x2t + (long long)(mt + k0) * TS * PW, kBlock,
+                         &rfull[ri_slot], pol_rb);
         }
         ++r_issued;
         if (++ri_slot == XST) ri_slot = 0;
@@ -668,8 +678,9 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
             fence_async_shared();
             __syncwarp();
             if (lane == 0) {
-              tma_store_2d(&J->maps[5], ob, mt - (s + 1) * R, c0);
-              if (mt + s * R < n) tma_store_2d(&J->maps[5], ob + 2 * BOX, mt + s * R, c0);
+              tma_store_2d_hint(&J->maps[5], ob, mt - (s + 1) * R, c0, pol_out);
+              if (mt + s * R < n)
+                tma_store_2d_hint(&J->maps[5], ob + 2 * BOX, mt + s * R, c0, pol_out);
               bulk_commit();
             }
           } else {
@@ -680,8 +691,9 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
               fence_async_shared();
               __syncwarp();
               if (lane == 0) {
-                tma_store_2d(&J->maps[6], ob, mt - (s + 1) * R, c0);
-                if (mt + (s - 1) * R < n) tma_store_2d(&J->maps[6], ob + 2 * BOX, mt + (s - 1) * R, c0);
+                tma_store_2d_hint(&J->maps[6], ob, mt - (s + 1) * R, c0, pol_out);
+                if (mt + (s - 1) * R < n)
+                  tma_store_2d_hint(&J->maps[6], ob + 2 * BOX, mt + (s - 1) * R, c0, pol_out);
                 bulk_commit();
               }
               o_buf ^= 1;
@@ -694,11 +706,11 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
           F *const p = JG.x + (long long)c2 * inner * n + c0 + sys + (long long)row0 * inner;
           if (part == 0 || mt + (s + 1) * R <= n) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) p[r * step] = xk[r];
+            for (int r = 0; r < R; ++r) st_hint(p + r * step, xk[r], pol_out);
           } else {  // the lower half's last stages end in virtual rows
 #pragma unroll
             for (int r = 0; r < R; ++r)
-              if (row0 + r < n) p[r * step] = xk[r];
+              if (row0 + r < n) st_hint(p + r * step, xk[r], pol_out);
           }
         }
       }
