@@ -11,13 +11,18 @@
 // -- is ignored, as on every other path.
 //
 // The Tensor-Memory kernel (n <= 256 in FP64, n <= 512 in FP32):
-//  * one CTA per SM: warps 0..3 solve, warp 4 builds the table.  A consumer
-//    warp owns 32 lines at a time (one per lane), streams their right-hand
-//    sides through a ring of TMA tiles {R rows x 32 lines} that it refills
-//    itself, keeps x2 of every row in its TMEM lane quarter (one tcgen05.st of
-//    16 columns per stage) and writes x back (directly along y/z, through a
-//    64-byte-swizzled shared tile and TMA stores along x).  HBM traffic is the
-//    algorithmic 2 x sizeof(F) per point.
+//  * one CTA per SM: for each TMEM lane quarter c, warp c runs the forward
+//    substitution and warp 4 + c the back substitution of the same tiles, one
+//    tile behind; warp 8 builds the table.  A tile is 32 lines (one per
+//    lane).  The forward warp streams their right-hand sides through a ring
+//    of TMA tiles {R rows x 32 lines} (along x: 128-byte rows, 128-byte
+//    swizzle) that it refills itself and keeps x2 of every row in its TMEM
+//    lane quarter (one tcgen05.st of 32 columns per stage); the back
+//    substitution reads it back and writes x (directly along y/z, through a
+//    swizzled shared tile and TMA stores along x).  Consecutive tiles fill
+//    TMEM blocks in opposite orders and a progress word hands blocks over, as
+//    in tmem_kernels.cu.  HBM traffic is the algorithmic 2 x sizeof(F) per
+//    point; loads and stores carry an evict-first L2 policy.
 //  * The builder warp loads line 0's coefficients, masks them and runs the
 //    serial recurrence into a shared-memory table, publishing it R rows at a
 //    time; consumers on their first tile follow it row block by row block.
@@ -44,10 +49,9 @@ constexpr int NCONS = 4;            // consumer warps: one per TMEM lane quarter
 constexpr uint32_t kTmemCols = 512;
 constexpr int kCacheMagic = 0x5f4a4355;  // table layout [e | a | inv | du2 | dw2]
 
-// A TMA box row is 64 bytes: RB rows of one line along x (64-byte swizzle).
-template <typename F> constexpr int sf_box_rows() { return 64 / (int)sizeof(F); }
-// A stage is two box rows: R = 16 (FP64) / 32 (FP32) rows, 32 TMEM columns.
-template <typename F> constexpr int sf_rows_per_stage() { return 2 * sf_box_rows<F>(); }
+// A stage is R = 16 (FP64) / 32 (FP32) rows, 128 bytes of a line along x
+// (one TMA tile {R rows, 32 lines}, 128-byte swizzle), 32 TMEM columns.
+template <typename F> constexpr int sf_rows_per_stage() { return 128 / (int)sizeof(F); }
 
 // TMEM holds x2 for n_pad = R ceil(n / R) rows: 2 columns per FP64 row.
 template <typename F> constexpr int sf_max_rows() {
@@ -55,13 +59,11 @@ template <typename F> constexpr int sf_max_rows() {
 }
 
 template <typename F, bool CONTIG, int ST> struct SfGeom {
-  static constexpr int RB = sf_box_rows<F>();
   static constexpr int R = sf_rows_per_stage<F>();
-  static constexpr int BOXE = RB * SL;                    // elements per x box (along x)
   static constexpr int SE = R * SL;                       // elements per stage
   static constexpr int OBE = CONTIG ? 2 * SE : 0;         // output tiles (2 buffers)
   static constexpr size_t kData = (size_t)(ST * SE + OBE) * sizeof(F);
-  static constexpr size_t kCons = (kData + ST * 8 + 1023) / 1024 * 1024;
+  static constexpr size_t kCons = (kData + (ST + 2) * 8 + 1023) / 1024 * 1024;
   static constexpr int kTabRows = sf_max_rows<F>();
   // table [e | a | inv | du2 | dw2], line-0 inputs, cached inputs: 3 x 5 rows
   static constexpr size_t kTable = (size_t)15 * kTabRows * sizeof(F);
@@ -69,7 +71,9 @@ template <typename F, bool CONTIG, int ST> struct SfGeom {
   // at least 116 KB, so that one CTA holds an SM (and all of its TMEM)
   static constexpr size_t kSmem = kUsed > 118784 ? kUsed : 118784;
   static constexpr int kCols = R * (int)sizeof(F) / 4;    // TMEM columns per stage (32)
+  static constexpr int NB = (int)kTmemCols / kCols;       // TMEM blocks of one stage each
   static_assert(kCols == 32, "32 TMEM columns per stage");
+  static_assert(kSmem <= 232448, "shared memory per CTA");
 };
 
 // The cache at the end of the caller's buffer:
@@ -121,7 +125,7 @@ __device__ __forceinline__ bool wait_table(volatile int *ready, int rows) {
 }
 
 template <typename F, bool CONTIG, int ST>
-__global__ void __launch_bounds__(32 * (NCONS + 1), 1)
+__global__ void __launch_bounds__(32 * (2 * NCONS + 1), 1)
 sf_tmem_kernel(const __grid_constant__ CUtensorMap xmap, const F *__restrict__ ds,
                const F *__restrict__ dl, const F *__restrict__ d, const F *__restrict__ du,
                const F *__restrict__ dw, F *__restrict__ x, unsigned char *__restrict__ cache,
@@ -129,7 +133,7 @@ sf_tmem_kernel(const __grid_constant__ CUtensorMap xmap, const F *__restrict__ d
                int *__restrict__ status_word) {
   using G = SfGeom<F, CONTIG, ST>;
   using V2 = typename Vec2<F>::T;
-  constexpr int RB = G::RB, R = G::R, BOXE = G::BOXE, SE = G::SE;
+  constexpr int R = G::R, SE = G::SE, NB = G::NB;
   constexpr int EPC = 16 / (int)sizeof(F);
   constexpr int TR = G::kTabRows;
 
@@ -144,14 +148,54 @@ sf_tmem_kernel(const __grid_constant__ CUtensorMap xmap, const F *__restrict__ d
   unsigned char *const tail = base + NCONS * G::kCons + G::kTable;
   uint32_t *const tmem_slot = reinterpret_cast<uint32_t *>(tail);
   volatile int *const ready = reinterpret_cast<volatile int *>(tail + 16);
+  volatile int *const stop = reinterpret_cast<volatile int *>(tail + 32);  // [NCONS]
   uint64_t *const cbar = reinterpret_cast<uint64_t *>(tail + 64);
+  int *const prog = reinterpret_cast<int *>(tail + 96);                    // [NCONS]
+
+  // The builder warp starts first: the table cache's bulk copies and the
+  // gather of line 0's coefficients (every load of a lane issued before any
+  // is used; rows lane + 32 j of each array) go out before the solving
+  // warps' ring loads, which they would otherwise queue behind.
+  constexpr int PL = (TR + 31) / 32;
+  const bool builder = warp == 2 * NCONS;
+  const long long stride = CONTIG ? 1 : inner;  // line 0's row stride
+  SfCacheHeader *const hdr = reinterpret_cast<SfCacheHeader *>(cache);
+  F *const c_in = cache ? reinterpret_cast<F *>(cache + 128) : nullptr;
+  F *const c_tab = c_in ? c_in + 5 * (long long)n_pad : nullptr;
+  F v[5][PL];
+  bool same = false;
+  if (builder) {
+    if (cache != nullptr && lane == 0) {
+      const unsigned comp = (unsigned)(n_pad * sizeof(F));
+      mbar_init(cbar, 1);
+      mbar_init_fence();
+      mbar_expect_tx(cbar, 10u * comp);
+      for (int q = 0; q < 5; ++q) {
+        bulk_load(cin + q * TR, c_in + (long long)q * n_pad, comp, cbar);
+        bulk_load(tab + q * TR, c_tab + (long long)q * n_pad, comp, cbar);
+      }
+    }
+    const F *const src[5] = {ds, dl, d, du, dw};
+#pragma unroll
+    for (int q = 0; q < 5; ++q)
+#pragma unroll
+      for (int j = 0; j < PL; ++j) {
+        const int i = lane + 32 * j;
+        v[q][j] = i < n ? src[q][(long long)i * stride] : F(0);
+      }
+    if (cache != nullptr) {
+      const volatile SfCacheHeader *vh = hdr;
+      same = vh->magic == kCacheMagic && vh->n == n && vh->elem == (int)sizeof(F);
+    }
+  }
 
   if (threadIdx.x == 0) {
     for (int c = 0; c < NCONS; ++c) {
       uint64_t *f = reinterpret_cast<uint64_t *>(base + c * G::kCons + G::kData);
-      for (int s = 0; s < ST; ++s) mbar_init(&f[s], 1);
+      for (int s = 0; s < ST + 2; ++s) mbar_init(&f[s], 1);
+      stop[c] = 0;
+      prog[c] = 0;
     }
-    mbar_init(cbar, 1);
     *ready = 0;
     mbar_init_fence();
   }
@@ -162,46 +206,15 @@ sf_tmem_kernel(const __grid_constant__ CUtensorMap xmap, const F *__restrict__ d
   const uint32_t tmem_base = *tmem_slot;
 
   // ================================ builder =================================
-  if (warp == NCONS) {
-    const long long stride = CONTIG ? 1 : inner;  // line 0's row stride
-    SfCacheHeader *hdr = reinterpret_cast<SfCacheHeader *>(cache);
-    F *const c_in = cache ? reinterpret_cast<F *>(cache + 128) : nullptr;
-    F *const c_tab = c_in ? c_in + 5 * (long long)n_pad : nullptr;
-    const unsigned comp = (unsigned)(n_pad * sizeof(F));
-    // the cached inputs and table come in by bulk copy while the lanes gather
-    // line 0's coefficients
-    if (cache != nullptr && lane == 0) {
-      mbar_expect_tx(cbar, 10u * comp);
-      for (int q = 0; q < 5; ++q) {
-        bulk_load(cin + q * TR, c_in + (long long)q * n_pad, comp, cbar);
-        bulk_load(tab + q * TR, c_tab + (long long)q * n_pad, comp, cbar);
-      }
-    }
-    bool same = false;
-    if (cache != nullptr) {
-      const volatile SfCacheHeader *vh = hdr;
-      same = vh->magic == kCacheMagic && vh->n == n && vh->elem == (int)sizeof(F);
-    }
+  if (builder) {
     const int total = 5 * n_pad;
-    constexpr int GB = 16;  // independent loads in flight per lane
-    for (int k0 = 0; k0 < total; k0 += 32 * GB) {
-      F v[GB];
 #pragma unroll
-      for (int j = 0; j < GB; ++j) {
-        const int k = k0 + j * 32 + lane;
-        const int q = k / n_pad, i = k - q * n_pad;
-        const F *src = q == 0 ? ds : q == 1 ? dl : q == 2 ? d : q == 3 ? du : dw;
-        v[j] = (k < total && i < n) ? src[(long long)i * stride] : F(0);
-      }
+    for (int q = 0; q < 5; ++q)
 #pragma unroll
-      for (int j = 0; j < GB; ++j) {
-        const int k = k0 + j * 32 + lane;
-        if (k < total) {
-          const int q = k / n_pad, i = k - q * n_pad;
-          coef[q * TR + i] = sf_mask<F>(q, i, n, v[j]);
-        }
+      for (int j = 0; j < PL; ++j) {
+        const int i = lane + 32 * j;
+        if (i < n_pad) coef[q * TR + i] = sf_mask<F>(q, i, n, v[q][j]);
       }
-    }
     bool copies_done = true;
     if (cache != nullptr) copies_done = __all_sync(0xffffffffu, mbar_wait(cbar, 0));
     if (!copies_done) {  // the table area may still be written: publish nothing
@@ -209,11 +222,15 @@ sf_tmem_kernel(const __grid_constant__ CUtensorMap xmap, const F *__restrict__ d
       return;
     }
     __syncwarp();
-    if (same)
-      for (int k = lane; k < total && same; k += 32) {
-        const int q = k / n_pad, i = k - q * n_pad;
-        same = same_bits(coef[q * TR + i], cin[q * TR + i]);
-      }
+    if (same) {  // the gathered (masked) coefficients against the cached ones
+#pragma unroll
+      for (int q = 0; q < 5; ++q)
+#pragma unroll
+        for (int j = 0; j < PL; ++j) {
+          const int i = lane + 32 * j;
+          if (i < n_pad) same &= same_bits(sf_mask<F>(q, i, n, v[q][j]), cin[q * TR + i]);
+        }
+    }
     if (__all_sync(0xffffffffu, same)) {  // cached table: already in place
       __threadfence_block();
       __syncwarp();
@@ -274,29 +291,33 @@ sf_tmem_kernel(const __grid_constant__ CUtensorMap xmap, const F *__restrict__ d
     return;
   }
 
-  // ================================ consumer ================================
-  const int cons = warp;
+  // ============================ solving warps ===============================
+  // warps 0..3 run the forward substitution of their lane quarter's tiles,
+  // warps 4..7 the back substitution, one tile behind (a warp reaches the
+  // TMEM lanes 32 (warp % 4) .. 32 (warp % 4) + 31)
+  const bool fwd = warp < NCONS;
+  const int cons = warp % NCONS;
   F *const ring = reinterpret_cast<F *>(base + cons * G::kCons);
   F *const obuf = ring + ST * SE;
   uint64_t *const full = reinterpret_cast<uint64_t *>(base + cons * G::kCons + G::kData);
+  uint64_t *const hfull = full + ST;  // [2]: a tile's x2 is in TMEM
   const uint32_t taddr = tmem_base + ((uint32_t)(cons * 32) << 16);
   const int n_stages = n_pad / R;
   const int gw = blockIdx.x * NCONS + cons;
   const int tw = gridDim.x * NCONS;
   const int my_tiles = gw < n_tiles ? (n_tiles - 1 - gw) / tw + 1 : 0;
   const long long total = (long long)my_tiles * n_stages;
+  const uint64_t pol_stream = l2_policy_first();  // every access is read or written once
 
-  // element offset of this lane's row r inside a stage
+  // element offset of this lane's row r inside a stage tile: along x a
+  // 128-byte row per line (128-byte swizzle), along y/z a row of 32 lines
   int off[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    if (CONTIG) {
-      const int rr = r % RB;
-      const int sw = (lane >> 1) & 3;  // 64-byte swizzle: 16-byte chunk ^= (line / 2) % 4
-      off[r] = (r / RB) * BOXE + lane * RB + ((rr / EPC) ^ sw) * EPC + rr % EPC;
-    } else {
+    if (CONTIG)
+      off[r] = lane * R + ((r / EPC) ^ (lane & 7)) * EPC + r % EPC;
+    else
       off[r] = r * SL + lane;
-    }
   }
 
   auto coords = [&](int tile, int &c0, int &c2) {
@@ -308,154 +329,222 @@ sf_tmem_kernel(const __grid_constant__ CUtensorMap xmap, const F *__restrict__ d
       c0 = (tile - c2 * tpr) * SL;
     }
   };
-  long long issued = 0;
-  int i_t = 0, i_g = 0, i_c0 = 0, i_c2 = 0;
-  auto issue = [&](int slot) {
-    if (issued >= total) return;
-    if (i_g == 0) coords(gw + i_t * tw, i_c0, i_c2);
-    if (lane == 0) {
-      F *dst = ring + slot * SE;
-      const int r0 = i_g * R;
-      if (CONTIG) {
-        const bool second = r0 + RB < n;  // else the second box lies wholly past row n
-        mbar_expect_tx(&full[slot], (unsigned)((second ? 2 : 1) * BOXE * sizeof(F)));
-        tma_load_2d(dst, &xmap, &full[slot], r0, i_c0);
-        if (second) tma_load_2d(dst + BOXE, &xmap, &full[slot], r0 + RB, i_c0);
-      } else {
+
+  if (fwd) {
+    // ------------------------- forward substitution --------------------------
+    // Tile ti stores stage g's x2 in TMEM block g (even ti) or NB-1-g (odd
+    // ti); the back substitution of the previous tile frees the blocks in the
+    // order this tile fills them and publishes prog[cons] = tile * 65536 +
+    // steps done.
+    long long issued = 0;
+    int i_t = 0, i_g = 0, i_c0 = 0, i_c2 = 0;
+    auto issue = [&](int slot) {
+      if (issued >= total) return;
+      if (i_g == 0) coords(gw + i_t * tw, i_c0, i_c2);
+      if (lane == 0) {
+        F *dst = ring + slot * SE;
         mbar_expect_tx(&full[slot], (unsigned)(SE * sizeof(F)));
-        tma_load_3d(dst, &xmap, &full[slot], i_c0, r0, i_c2);
+        if (CONTIG)
+          tma_load_2d_hint(dst, &xmap, &full[slot], i_g * R, i_c0, pol_stream);
+        else
+          tma_load_3d_hint(dst, &xmap, &full[slot], i_c0, i_g * R, i_c2, pol_stream);
       }
-    }
-    ++issued;
-    if (++i_g == n_stages) {
-      i_g = 0;
-      ++i_t;
-    }
-  };
-  for (int s = 0; s < ST; ++s) issue(s);
+      ++issued;
+      if (++i_g == n_stages) {
+        i_g = 0;
+        ++i_t;
+      }
+    };
+    for (int s = 0; s < ST; ++s) issue(s);
 
-  int slot = 0, o_buf = 0;
-  unsigned phase = 0;
-  long long consumed = 0;
-  bool timed_out = false;
-  const V2 *const t_e = reinterpret_cast<const V2 *>(tab);
-  const V2 *const t_a = reinterpret_cast<const V2 *>(tab + TR);
-  const V2 *const t_inv = reinterpret_cast<const V2 *>(tab + 2 * TR);
-  const V2 *const t_du2 = reinterpret_cast<const V2 *>(tab + 3 * TR);
-  const V2 *const t_dw2 = reinterpret_cast<const V2 *>(tab + 4 * TR);
-
-  for (int ti = 0; ti < my_tiles && !timed_out; ++ti) {
-    int c0, c2;
-    coords(gw + ti * tw, c0, c2);
-    const int count = CONTIG ? min(SL, n_sys - c0) : min(SL, inner - c0);
-    F p2 = F(0), p1 = F(0);
-    for (int g = 0; g < n_stages; ++g) {
-      const bool ok = (ti > 0 || wait_table(ready, (g + 1) * R)) &&
-                      mbar_wait(&full[slot], phase);
-      if (!__all_sync(0xffffffffu, ok)) {
-        timed_out = true;
-        break;
-      }
-      __threadfence_block();
-      F b[R];
-      const F *v = ring + slot * SE;
-#pragma unroll
-      for (int r = 0; r < R; ++r) b[r] = v[off[r]];
-      fence_async_shared();
-      __syncwarp();
-      ++consumed;
-      issue(slot);  // refill the slot just read
-      if (++slot == ST) {
-        slot = 0;
-        phase ^= 1u;
-      }
-      const int k0 = g * R;
-      if (k0 + R > n) {  // rows past n (not loaded, or zero-filled) contribute nothing
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-          if (k0 + r >= n) b[r] = F(0);
-      }
-      F e[R], a[R], inv[R];
-#pragma unroll
-      for (int j = 0; j < R / 2; ++j) {
-        const V2 ev = t_e[k0 / 2 + j], av = t_a[k0 / 2 + j], iv = t_inv[k0 / 2 + j];
-        e[2 * j] = ev.x; e[2 * j + 1] = ev.y;
-        a[2 * j] = av.x; a[2 * j + 1] = av.y;
-        inv[2 * j] = iv.x; inv[2 * j + 1] = iv.y;
-      }
-      uint32_t tv[32];
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        // y = (b - ds y2 - ddl y1) / dd, with e = ds / dd and a = ddl / dd
-        const F y = fma(-a[r], p1, fma(-e[r], p2, b[r] * inv[r]));
-        p2 = p1;
-        p1 = y;
-        put_x2<F>(tv, r, y);
-      }
-      tmem_store32(taddr + (uint32_t)(g * G::kCols), tv);
-    }
-    if (timed_out) break;
-    F s0 = F(0), s1 = F(0);  // x of the two rows below
-    for (int g = n_stages - 1; g >= 0; --g) {
-      const int k0 = g * R;
-      uint32_t tv[32];
-      tmem_load32(taddr + (uint32_t)(g * G::kCols), tv);
-      F u[R], w[R];
-#pragma unroll
-      for (int j = 0; j < R / 2; ++j) {
-        const V2 uv = t_du2[k0 / 2 + j], wv = t_dw2[k0 / 2 + j];
-        u[2 * j] = uv.x; u[2 * j + 1] = uv.y;
-        w[2 * j] = wv.x; w[2 * j + 1] = wv.y;
-      }
-      F xo[R];
-#pragma unroll
-      for (int r = R - 1; r >= 0; --r) {
-        const F xj = fma(-u[r], s0, fma(-w[r], s1, get_x2<F>(tv, r)));
-        s1 = s0;
-        s0 = xj;
-        xo[r] = xj;
-      }
-      if (CONTIG) {
-        F *const ob = obuf + o_buf * SE;
-        if (lane == 0) bulk_wait_read<1>();  // this buffer's previous stores have read it
-        __syncwarp();
-#pragma unroll
-        for (int r = 0; r < R; ++r) ob[off[r]] = xo[r];
-        fence_async_shared();
-        __syncwarp();
-        if (lane == 0) {
-          tma_store_2d(&xmap, ob, k0, c0);
-          if (k0 + RB < n) tma_store_2d(&xmap, ob + BOXE, k0 + RB, c0);
-          bulk_commit();
+    const V2 *const t_e = reinterpret_cast<const V2 *>(tab);
+    const V2 *const t_a = reinterpret_cast<const V2 *>(tab + TR);
+    const V2 *const t_inv = reinterpret_cast<const V2 *>(tab + 2 * TR);
+    const int free_blocks = NB - n_stages;  // blocks a tile never uses
+    int slot = 0, seen = 0, fail = 0, ti = 0;
+    unsigned phase = 0;
+    long long consumed = 0;
+    for (; ti < my_tiles; ++ti) {
+      const bool flip = (ti & 1) != 0;
+      F p2 = F(0), p1 = F(0);
+      for (int g = 0; g < n_stages; ++g) {
+        const bool ok = (ti > 0 || wait_table(ready, (g + 1) * R)) &&
+                        mbar_wait(&full[slot], phase);
+        if (!__all_sync(0xffffffffu, ok)) {
+          fail = 1;
+          break;
         }
-        o_buf ^= 1;
-      } else if (lane < count) {
-        F *const p = x + (long long)c2 * inner * n + c0 + lane;
-        if (k0 + R <= n) {
+        if (ti == 0) __threadfence_block();  // the table rows just published
+        F b[R];
+        const F *v = ring + slot * SE;
+        if (CONTIG) {  // rows 2j, 2j+1 share a 16-byte chunk
 #pragma unroll
-          for (int r = 0; r < R; ++r) p[(long long)(k0 + r) * inner] = xo[r];
+          for (int j = 0; j < R / 2; ++j) {
+            const V2 pv = *reinterpret_cast<const V2 *>(v + off[2 * j]);
+            b[2 * j] = pv.x;
+            b[2 * j + 1] = pv.y;
+          }
         } else {
 #pragma unroll
+          for (int r = 0; r < R; ++r) b[r] = v[off[r]];
+        }
+        fence_async_shared();
+        __syncwarp();
+        ++consumed;
+        issue(slot);  // refill the slot just read
+        if (++slot == ST) {
+          slot = 0;
+          phase ^= 1u;
+        }
+        const int k0 = g * R;
+        if (k0 + R > n) {  // rows past n (zero-filled) contribute nothing
+#pragma unroll
           for (int r = 0; r < R; ++r)
-            if (k0 + r < n) p[(long long)(k0 + r) * inner] = xo[r];
+            if (k0 + r >= n) b[r] = F(0);
+        }
+        uint32_t tv[32];
+#pragma unroll
+        for (int j = 0; j < R / 2; ++j) {
+          const V2 ev = t_e[k0 / 2 + j], av = t_a[k0 / 2 + j], iv = t_inv[k0 / 2 + j];
+          // y = (b - ds y2 - ddl y1) / dd, with e = ds / dd and a = ddl / dd
+          const F y0 = fma(-av.x, p1, fma(-ev.x, p2, b[2 * j] * iv.x));
+          const F y1 = fma(-av.y, y0, fma(-ev.y, p1, b[2 * j + 1] * iv.y));
+          p2 = y0;
+          p1 = y1;
+          put_x2<F>(tv, 2 * j, y0);
+          put_x2<F>(tv, 2 * j + 1, y1);
+        }
+        // wait (lane 0, bounded) until the previous tile has read this block
+        const int need = (ti - 1) * 65536 + max(0, g + 1 - free_blocks);
+        int go = 1;
+        if (lane == 0 && seen < need) {
+          seen = ld_acquire_shared(&prog[cons]);
+          if (seen < need) {
+            const unsigned long long t0 = global_ns();
+            for (;;) {
+              __nanosleep(32);
+              seen = ld_acquire_shared(&prog[cons]);
+              if (seen >= need) break;
+              if (stop[cons] != 0) {
+                go = 2;
+                break;
+              }
+              if (global_ns() - t0 > 2000000000ull) {
+                go = 0;
+                break;
+              }
+            }
+          }
+        }
+        go = __shfl_sync(0xffffffffu, go, 0);
+        if (go != 1) {
+          fail = go == 0 ? 1 : 2;
+          break;
+        }
+        tmem_fence_after_sync();
+        const int blk = flip ? NB - 1 - g : g;
+        tmem_store32(taddr + (uint32_t)(blk * G::kCols), tv);
+      }
+      if (fail) break;
+      tmem_fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&hfull[ti & 1]);
+    }
+    if (fail) {
+      stop[cons] = 1;
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&hfull[ti & 1]);  // wake the back substitution
+      // drain the loads this warp issued (bounded waits)
+      for (; consumed < issued; ++consumed) {
+        if (!mbar_wait(&full[slot], phase)) break;
+        if (++slot == ST) {
+          slot = 0;
+          phase ^= 1u;
         }
       }
+      if (fail == 1 && lane == 0) atomicOr(status_word, STATUS_TIMEOUT_BIT);
     }
-  }
-  if (timed_out) {
-    // drain the loads this warp issued (bounded waits)
-    for (; consumed < issued; ++consumed) {
-      if (!mbar_wait(&full[slot], phase)) break;
-      if (++slot == ST) {
-        slot = 0;
-        phase ^= 1u;
+  } else {
+    // --------------------------- back substitution ---------------------------
+    const V2 *const t_du2 = reinterpret_cast<const V2 *>(tab + 3 * TR);
+    const V2 *const t_dw2 = reinterpret_cast<const V2 *>(tab + 4 * TR);
+    int o_buf = 0, fail = 0;
+    for (int ti = 0; ti < my_tiles; ++ti) {
+      int c0, c2;
+      coords(gw + ti * tw, c0, c2);
+      const int count = CONTIG ? min(SL, n_sys - c0) : min(SL, inner - c0);
+      const bool flip = (ti & 1) != 0;
+      if (!__all_sync(0xffffffffu, mbar_wait(&hfull[ti & 1], (unsigned)(ti >> 1) & 1u))) {
+        fail = 1;
+        break;
       }
+      if (stop[cons] != 0) {
+        fail = 2;
+        break;
+      }
+      tmem_fence_after_sync();
+      F s0 = F(0), s1 = F(0);  // x of the two rows below
+      for (int g = n_stages - 1; g >= 0; --g) {
+        const int k0 = g * R;
+        const int blk = flip ? NB - 1 - g : g;
+        uint32_t tv[32];
+        tmem_load32(taddr + (uint32_t)(blk * G::kCols), tv);
+        // the block is free for the next tile's forward substitution
+        tmem_fence_before_sync();
+        __syncwarp();
+        if (lane == 0) st_release_shared(&prog[cons], ti * 65536 + (n_stages - g));
+        F xo[R];
+#pragma unroll
+        for (int j = R / 2 - 1; j >= 0; --j) {
+          const V2 uv = t_du2[k0 / 2 + j], wv = t_dw2[k0 / 2 + j];
+          const F x1 = fma(-uv.y, s0, fma(-wv.y, s1, get_x2<F>(tv, 2 * j + 1)));
+          const F x0 = fma(-uv.x, x1, fma(-wv.x, s0, get_x2<F>(tv, 2 * j)));
+          s1 = x1;
+          s0 = x0;
+          xo[2 * j + 1] = x1;
+          xo[2 * j] = x0;
+        }
+        if (CONTIG) {
+          F *const ob = obuf + o_buf * SE;
+          if (lane == 0) bulk_wait_read<1>();  // this buffer's previous store has read it
+          __syncwarp();
+#pragma unroll
+          for (int j = 0; j < R / 2; ++j) {
+            V2 pv;
+            pv.x = xo[2 * j];
+            pv.y = xo[2 * j + 1];
+            *reinterpret_cast<V2 *>(ob + off[2 * j]) = pv;
+          }
+          fence_async_shared();
+          __syncwarp();
+          if (lane == 0) {
+            tma_store_2d_hint(&xmap, ob, k0, c0, pol_stream);
+            bulk_commit();
+          }
+          o_buf ^= 1;
+        } else if (lane < count) {
+          F *const p = x + (long long)c2 * inner * n + c0 + lane;
+          if (k0 + R <= n) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) st_hint(p + (long long)(k0 + r) * inner, xo[r], pol_stream);
+          } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+              if (k0 + r < n) st_hint(p + (long long)(k0 + r) * inner, xo[r], pol_stream);
+          }
+        }
+      }
+      if (lane == 0) st_release_shared(&prog[cons], (ti + 1) * 65536);
     }
-    if (lane == 0) atomicOr(status_word, STATUS_TIMEOUT_BIT);
+    if (fail) {
+      stop[cons] = 1;
+      if (fail == 1 && lane == 0) atomicOr(status_word, STATUS_TIMEOUT_BIT);
+    }
+    if (CONTIG && lane == 0) bulk_wait<0>();
   }
-  if (CONTIG && lane == 0) bulk_wait<0>();
+  // the solving warps are done with Tensor Memory: warp 0 frees it
   tmem_fence_before_sync();
-  asm volatile("bar.sync 1, %0;\n" ::"n"(32 * NCONS) : "memory");
+  asm volatile("bar.sync 1, %0;\n" ::"n"(64 * NCONS) : "memory");
   tmem_fence_after_sync();
   if (warp == 0) tmem_dealloc(tmem_base, kTmemCols);
 }
@@ -534,7 +623,7 @@ bool sf_encode(CUtensorMap *m, const F *ptr, const Lines &L, bool contig, int R)
     const cuuint32_t box[2] = {(cuuint32_t)R, (cuuint32_t)SL};
     const cuuint32_t es[2] = {1, 1};
     r = fn(m, dt, 2, const_cast<F *>(ptr), dims, strides, box, es,
-           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   } else {
     const cuuint64_t dims[3] = {(cuuint64_t)L.inner, (cuuint64_t)L.n,
@@ -563,7 +652,7 @@ cudaError_t sf_tmem_launch(const SolveArgs<F> &a, int sm_count, size_t usable_bu
                            cudaStream_t stream) {
   using G = SfGeom<F, CONTIG, ST>;
   CUtensorMap xmap;
-  if (!sf_encode<F>(&xmap, a.x, a.L, CONTIG, CONTIG ? G::RB : G::R)) return cudaErrorInvalidValue;
+  if (!sf_encode<F>(&xmap, a.x, a.L, CONTIG, G::R)) return cudaErrorInvalidValue;
   auto kern = sf_tmem_kernel<F, CONTIG, ST>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)G::kSmem);
@@ -584,7 +673,7 @@ cudaError_t sf_tmem_launch(const SolveArgs<F> &a, int sm_count, size_t usable_bu
   }
   const long long need = (n_tiles + NCONS - 1) / NCONS;
   const int grid = (int)(need < sm_count ? need : sm_count);
-  kern<<<grid, 32 * (NCONS + 1), G::kSmem, stream>>>(xmap, a.ds, a.dl, a.d, a.du, a.dw, a.x,
+  kern<<<grid, 32 * (2 * NCONS + 1), G::kSmem, stream>>>(xmap, a.ds, a.dl, a.d, a.du, a.dw, a.x,
                                                      cache, n, n_pad, inner, tpr,
                                                      (int)a.L.n_sys, (int)n_tiles, a.status);
   return cudaGetLastError();
@@ -596,7 +685,7 @@ template <typename F, bool CONTIG, int ST> int sf_occ() {
   int blocks = 0;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)G::kSmem) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, 32 * (NCONS + 1),
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, 32 * (2 * NCONS + 1),
                                                     G::kSmem) != cudaSuccess) {
     cudaGetLastError();
     return 0;
