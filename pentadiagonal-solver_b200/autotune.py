@@ -26,8 +26,11 @@ import pentadsolver as ps
 
 # (label, tuning spec, algorithm, pcr lanes)
 SOLVE_CANDIDATES = [
+    ("tmem 2/4", "tmem=2,4", "thomas-pcr", 2),
+    ("tmem 2/3", "tmem=2,3", "thomas-pcr", 2),
     ("tmem 3/4", "tmem=3,4", "thomas-pcr", 2),
     ("tmem 3/3", "tmem=3,3", "thomas-pcr", 2),
+    ("tmem 3/2", "tmem=3,2", "thomas-pcr", 2),
     ("tmem 4/3", "tmem=4,3", "thomas-pcr", 2),
     ("tma", "no-tmem", "thomas-pcr", 2),
     ("cp.async P2", "no-tma", "thomas-pcr", 2),

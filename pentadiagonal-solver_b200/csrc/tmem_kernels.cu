@@ -351,16 +351,20 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
     // in the order that frees exactly the ones this tile fills first, and
     // publishes its progress in prog[cons] = tile * 65536 + steps done: block
     // b of this tile is free once that tile has done b's share of its steps.
-    int ld[R];  // element offset, inside a stage, of this lane's r-th row
+    // element offset, inside a stage, of this lane's r-th row (strided), or
+    // of the 16-byte chunk holding its rows 2j and 2j+1 (along x: a line's
+    // rows are contiguous, two to a chunk, so they are read in pairs)
+    int ld[CONTIG ? R / 2 : R];
+    if constexpr (CONTIG) {
+      const int sw = (sys >> 1) & 3;  // 64-byte swizzle: 16-byte chunk ^= (line / 2) % 4
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int rl = part ? (R - 1 - r) : r;
-      if (CONTIG) {
-        const int sw = (sys >> 1) & 3;  // 64-byte swizzle: 16-byte chunk ^= (row / 2) % 4
-        ld[r] = part * BOX + sys * R + ((rl / EPC) ^ sw) * EPC + rl % EPC;
-      } else {
-        ld[r] = part * BOX + rl * TS + sys;
+      for (int j = 0; j < R / 2; ++j) {
+        const int e = part ? (R - 2 - 2 * j) : 2 * j;  // the pair's even row in the tile
+        ld[j] = part * BOX + sys * R + ((e / EPC) ^ sw) * EPC + e % EPC;
       }
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) ld[r] = part * BOX + (part ? (R - 1 - r) : r) * TS + sys;
     }
     const uint64_t pol_x2 = l2_policy_last();  // read back soon: keep in L2
     int slot = 0, cursor = 0, n_prev = 0, seen = 0;
@@ -393,10 +397,22 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         }
         const F *v = ring + slot * SE;
         F a[R][6];
+        if constexpr (CONTIG) {
+          // the lower half runs its tile backwards: the pair's odd row first
 #pragma unroll
-        for (int r = 0; r < R; ++r)
+          for (int q = 0; q < 6; ++q)
 #pragma unroll
-          for (int q = 0; q < 6; ++q) a[r][q] = v[ld[r] + q * 2 * BOX];
+            for (int j = 0; j < R / 2; ++j) {
+              const V2 pv = *reinterpret_cast<const V2 *>(v + ld[j] + q * 2 * BOX);
+              a[2 * j][q] = part ? pv.y : pv.x;
+              a[2 * j + 1][q] = part ? pv.x : pv.y;
+            }
+        } else {
+#pragma unroll
+          for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int q = 0; q < 6; ++q) a[r][q] = v[ld[r] + q * 2 * BOX];
+        }
         if (g * R < nvp + 2) {  // virtual rows, and couplings that leave the line
 #pragma unroll
           for (int r = 0; r < R; ++r) {
@@ -511,20 +527,29 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   } else {
     // ========================= back-substitution ============================
     // Along x the results of two steps leave together as one tile of 2R rows
-    // (128-byte rows, 128-byte swizzle) per half; st2[r] is the offset, in a
-    // half's tile, of this lane's r-th row of an even step (an odd step's is
-    // st2[r] ^ R: its rows are the other R of the tile).  A last step without
-    // a partner uses R-row tiles (64-byte swizzle, offsets st1).
-    int st1[R], st2[R];
+    // (128-byte rows, 128-byte swizzle) per half, written two rows at a time
+    // (st2 below; an odd step's offsets are an even step's ^ R: its rows are
+    // the other R of the tile).  A last step without a partner uses R-row
+    // tiles (64-byte swizzle, offsets st1).
+    int st1[R], st2[R / 2];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       if (CONTIG) {
         const int rs = part ? r : (R - 1 - r);
         st1[r] = part * 2 * BOX + sys * R + ((rs / EPC) ^ ((sys >> 1) & 3)) * EPC + rs % EPC;
-        const int rr = part ? r : (2 * R - 1 - r);
-        st2[r] = part * 2 * BOX + sys * 2 * R + ((rr / EPC) ^ (sys & 7)) * EPC + rr % EPC;
       } else {
-        st1[r] = st2[r] = 0;
+        st1[r] = 0;
+      }
+    }
+    // rows 2j and 2j+1 of a step share a 16-byte chunk of the 2R-row tile:
+    // st2[j] is the chunk's even row (the upper half writes its rows downwards)
+#pragma unroll
+    for (int j = 0; j < R / 2; ++j) {
+      if (CONTIG) {
+        const int rr = part ? 2 * j : (2 * R - 2 - 2 * j);
+        st2[j] = part * 2 * BOX + sys * 2 * R + ((rr / EPC) ^ (sys & 7)) * EPC + rr % EPC;
+      } else {
+        st2[j] = 0;
       }
     }
     const bool drop = (flags & 1) != 0;
@@ -686,7 +711,12 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
           } else {
             const int odd = (s & 1) ? R : 0;
 #pragma unroll
-            for (int r = 0; r < R; ++r) ob[st2[r] ^ odd] = xk[r];
+            for (int j = 0; j < R / 2; ++j) {
+              V2 pv;
+              pv.x = part ? xk[2 * j] : xk[2 * j + 1];
+              pv.y = part ? xk[2 * j + 1] : xk[2 * j];
+              *reinterpret_cast<V2 *>(ob + (st2[j] ^ odd)) = pv;
+            }
             if (odd) {  // steps s - 1 and s: rows [mt - (s+1) R, mt - (s-1) R) of each half
               fence_async_shared();
               __syncwarp();
@@ -872,19 +902,24 @@ template <typename F, bool CONTIG, bool W2S, int ST, int XST> int tmem_occ() {
 
 // (type, contiguous, dw2 in the buffer, forward stages, read-back stages); for
 // each (type, layout, mode) the first variant is the default.  Batched
-// launches use the default variants.
+// launches use the default variants.  Along x two forward stages beat three:
+// fewer 64-byte requests in flight per line keep HBM row hits up (measured at
+// 256^3 and 512^3); the strided directions want three.
 #define PENTA_TMEM_CONFIGS(X)   \
+  X(double, true, false, 2, 4)  \
   X(double, true, false, 3, 4)  \
   X(double, true, false, 3, 3)  \
   X(double, false, false, 3, 4) \
   X(double, false, false, 3, 3) \
-  X(double, false, false, 4, 2) \
-  X(double, false, false, 4, 1) \
+  X(double, false, false, 2, 4) \
+  X(double, true, true, 2, 3)   \
   X(double, true, true, 3, 2)   \
   X(double, false, true, 3, 4)  \
+  X(float, true, false, 2, 4)   \
   X(float, true, false, 3, 4)   \
   X(float, false, false, 3, 4)  \
   X(float, false, false, 4, 3)  \
+  X(float, true, true, 2, 3)    \
   X(float, true, true, 3, 2)    \
   X(float, false, true, 3, 4)
 
@@ -978,10 +1013,10 @@ cudaError_t launch_tmem_batch(const void *device_jobs, int n_jobs, int total_til
   const TmemJob<F> *jobs = static_cast<const TmemJob<F> *>(device_jobs);
   const int flags = discard ? 1 : 0;
   if (contig && !w2s)
-    return tmem_launch_raw<F, true, false, 3, 4, true>(none, jobs, n_jobs, total_tiles, flags,
+    return tmem_launch_raw<F, true, false, 2, 4, true>(none, jobs, n_jobs, total_tiles, flags,
                                                        sm_count, status, stream);
   if (contig && w2s)
-    return tmem_launch_raw<F, true, true, 3, 2, true>(none, jobs, n_jobs, total_tiles, flags,
+    return tmem_launch_raw<F, true, true, 2, 3, true>(none, jobs, n_jobs, total_tiles, flags,
                                                       sm_count, status, stream);
   if (!w2s)
     return tmem_launch_raw<F, false, false, 3, 4, true>(none, jobs, n_jobs, total_tiles, flags,
