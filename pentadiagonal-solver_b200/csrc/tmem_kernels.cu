@@ -242,10 +242,16 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
     int slot = 0, use = 0, cursor = 0, fenced = -1;
     Geo JG;
     load_geo(job_of(gw, cursor), JG);
+    const F *arrs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     for (int ti = 0; ti < my_tiles; ++ti) {
       const int t = gw + ti * tw;
       const TmemJob<F> *J = job_of(t, cursor);
-      if (J != JG.J) load_geo(J, JG);
+      if (J != JG.J || ti == 0) {
+        load_geo(J, JG);
+        if (!JG.tma)
+#pragma unroll
+          for (int q = 0; q < 6; ++q) arrs[q] = J->arr[q];
+      }
       const bool tma = JG.tma != 0;
       if (BATCH && cursor != fenced) {  // a new grid: its maps, and the next grid's
         if (lane == 0) {
@@ -301,33 +307,42 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
           }
         } else {
           // the same tiles, element by element; rows past n and lines past the
-          // grid read as zeros
-          for (int e = lane; e < 12 * BOX; e += 32) {
-            const int bx = e / BOX, idx = e - bx * BOX;
+          // grid read as zeros.  The 12 tiles unrolled: each one's array is
+          // a register (no job-table load per element).  Along x a lane copies
+          // row lane % R of lines lane / R + (32 / R) k; strided, line
+          // lane % 16 at rows lane / 16 + 2 k.
+          constexpr int K = BOX / 32;  // elements per lane per tile
+#pragma unroll
+          for (int bx = 0; bx < 12; ++bx) {
             const int q = bx >> 1, h = bx & 1;
-            int s, rr, doff;
+            const F *const src = h ? arrs[kMirror[q]] : arrs[q];
+            const int rbase = h ? r_dn : r_up;
+            F *const tdst = dst + bx * BOX;
             if (CONTIG) {
-              s = idx / R;
-              rr = idx - s * R;
-              doff = s * R + ((rr / EPC) ^ ((s >> 1) & 3)) * EPC + rr % EPC;
+              const int rr = lane % R;
+              const int row = rbase + rr;
+#pragma unroll 4
+              for (int k = 0; k < K; ++k) {
+                const int ls = lane / R + (32 / R) * k;
+                const bool valid = row < n && c0 + ls < JG.n_sys;
+                const int doff = ls * R + ((rr / EPC) ^ ((ls >> 1) & 3)) * EPC + rr % EPC;
+                cp_async_zfill<sizeof(F)>(tdst + doff,
+                                          valid ? src + (long long)(c0 + ls) * n + row : src,
+                                          valid);
+              }
             } else {
-              rr = idx / TS;
-              s = idx - rr * TS;
-              doff = idx;
+              const int ls = lane % TS;
+              const bool lvalid = c0 + ls < inner;
+              const F *const lp = src + (long long)c2 * inner * n + c0 + ls;
+#pragma unroll 4
+              for (int k = 0; k < K; ++k) {
+                const int rr = lane / TS + 2 * k;
+                const int row = rbase + rr;
+                const bool valid = lvalid && row < n;
+                cp_async_zfill<sizeof(F)>(tdst + rr * TS + ls,
+                                          valid ? lp + (long long)row * inner : src, valid);
+              }
             }
-            const int row = h ? (r_dn + rr) : (r_up + rr);
-            const int which = h ? (q == 5 ? 5 : 4 - q) : q;
-            const F *src = J->arr[which];
-            bool valid = row < n;
-            long long off;
-            if (CONTIG) {
-              valid = valid && c0 + s < JG.n_sys;
-              off = (long long)(c0 + s) * n + row;
-            } else {
-              valid = valid && c0 + s < inner;
-              off = (long long)c2 * inner * n + (long long)row * inner + c0 + s;
-            }
-            cp_async_zfill<sizeof(F)>(dst + bx * BOX + doff, valid ? src + off : src, valid);
           }
           cp_async_mbar_arrive(&full[slot]);
         }
