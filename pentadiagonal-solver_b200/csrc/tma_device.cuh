@@ -154,6 +154,14 @@ __device__ __forceinline__ void tma_store_2d_hint(const CUtensorMap *map, const 
       "r"(smem_u32(src)), "r"(c0), "r"(c1), "l"(pol)
       : "memory");
 }
+__device__ __forceinline__ void tma_store_3d_hint(const CUtensorMap *map, const void *src, int c0,
+                                                  int c1, int c2, uint64_t pol) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group.L2::cache_hint"
+      " [%0, {%2, %3, %4}], [%1], %5;\n" ::"l"(reinterpret_cast<uint64_t>(map)),
+      "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "l"(pol)
+      : "memory");
+}
 __device__ __forceinline__ void bulk_load_hint(void *dst, const void *src, unsigned bytes,
                                                uint64_t *bar, uint64_t pol) {
   asm volatile(

@@ -59,7 +59,7 @@ def shared_solve(co, solvedim, dims, buffer="default", check_status=True):
 
 
 SHAPES = [(64, 64, 64), (48, 20, 33), (40, 24, 18), (256, 3, 5), (6, 40, 21), (33, 17, 6),
-          (300, 5, 4), (5, 6, 300), (20, 36, 9)]
+          (300, 5, 4), (5, 6, 300), (20, 36, 9), (512, 6, 5), (18, 32, 20)]
 
 
 @pytest.mark.parametrize("dims", SHAPES)
@@ -73,13 +73,15 @@ def test_shared_fact_matches_oracle_every_direction(cuda, dims, dtype):
         ref = oracle_solution(co, solvedim)
         got, var = shared_solve(co, solvedim, dims)
         assert fwd_err(got, ref) <= FWD_TOL[dtype], (dims, solvedim, var)
-        # the Tensor-Memory kernel takes aligned lines of at most 256 (FP64) /
-        # 512 (FP32) rows; everything else uses the per-line kernel
+        # the Tensor-Memory kernel takes aligned lines split into two halves of
+        # m = R ceil(n / 2R) rows, m <= 256 (FP64) / 512 (FP32), with two real
+        # rows in the lower half; everything else uses the per-line kernel
         n = dims[solvedim]
         inner = int(np.prod(dims[:solvedim]))
-        r = 2 * (64 // eb)  # rows per stage
+        r = 128 // eb  # rows per stage
+        m = r * -(-n // (2 * r))
         aligned = (n * eb) % 16 == 0 if solvedim == 0 else (inner > 1 and (inner * eb) % 16 == 0)
-        tm = aligned and r * -(-n // r) <= (256 if eb == 8 else 512)
+        tm = aligned and m <= (256 if eb == 8 else 512) and n - m >= 2
         assert ("tmem" in var) == tm, (dims, solvedim, var)
 
 
@@ -163,8 +165,10 @@ def test_shared_fact_environment_selector(cuda, monkeypatch):
     assert fwd_err(dv["x"].cpu().numpy(), ref) <= 1e-12
 
 
-def test_shared_fact_zero_pivot_is_reported(cuda):
-    dims = (16, 8, 8)
+@pytest.mark.parametrize("dims", [(16, 8, 8), (48, 8, 8)])
+def test_shared_fact_zero_pivot_is_reported(cuda, dims):
+    # (16, 8, 8): the per-line kernel; (48, 8, 8): the Tensor-Memory kernel,
+    # whose upper table meets the zero pivot at row 0
     co = shared_problem(dims, 0, 3, np.float64)
     co["d"][..., 0] = 0.0
     co["dl"][..., 1] = 0.0
