@@ -212,6 +212,31 @@ def run_ours(args):
     alg_bytes_step = BYTES_PER_POINT_AXIS * n ** 3 * 3 * ITERS
     value = world * alg_bytes_step / (ms_step * 1e-3) / 1e9
 
+    # ---- the same steps, each one CUDA graph of its 150 solves ----------------
+    from adi import AdiGraph
+
+    adi_graph = AdiGraph(*(d[k] for k in names), d["x"], iterations=ITERS, buffer=buf,
+                         handle=handle)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            adi_graph.replay()
+    torch.cuda.synchronize()
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        g0.record(stream)
+        for _ in range(args.steps):
+            adi_graph.replay()
+        g1.record(stream)
+    torch.cuda.synchronize()
+    graph_ms = g0.elapsed_time(g1) / args.steps
+    if world > 1:
+        t = torch.tensor([graph_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        graph_ms = float(t.item())
+    adi_graph.close()
+    del adi_graph
+
     # ---- end to end through the public API with host buffers ----------------
     # Every step is a fresh problem: its six arrays come from pinned host
     # memory and its result goes back.  Steps are pipelined as a serving loop
@@ -320,6 +345,9 @@ def run_ours(args):
                 "steps": e2e_steps,
                 "schedule": "pipelined: copies in of step k+1 and out of step k-1 overlap "
                             "the solves of step k (two device sets, two copy streams)"},
+        "graph": {"value": round(world * alg_bytes_step / (graph_ms * 1e-3) / 1e9, 2),
+                  "unit": "GB/s", "ms_per_step": round(graph_ms, 4),
+                  "note": "each step's 150 solves replayed as one CUDA graph (adi.AdiGraph)"},
         "gpu_launches": args.steps * ITERS * 3,
         "roofline": {
             "bound": "hbm",
