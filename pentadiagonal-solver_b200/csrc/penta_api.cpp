@@ -367,14 +367,14 @@ bool pick_tma_contig(Context &ctx, const SolveArgs<F> &a, size_t usable_buf,
 template <typename F>
 bool pick_tmem(Context &ctx, const SolveArgs<F> &a, bool contig, size_t usable_buf,
                TmemConfig &out, const std::string &variant) {
-  bool w2s = false;
-  if (!tmem_supported<F>(a, contig, usable_buf, w2s)) return false;
+  int fmode = 0;
+  if (!tmem_supported<F>(a, contig, usable_buf, fmode)) return false;
   int want[2] = {-1, -1};
   if (!variant.empty()) std::sscanf(variant.c_str(), "%d,%d", &want[0], &want[1]);
   const std::vector<TmemConfig> &all = tmem_configs<F>();
   for (size_t i = 0; i < all.size(); ++i) {
     const TmemConfig &c = all[i];
-    if (c.contig != contig || c.w2s != w2s) continue;
+    if (c.contig != contig || c.fmode != fmode) continue;
     if ((want[0] >= 0 && c.stages != want[0]) || (want[1] >= 0 && c.xstages != want[1]))
       continue;
     if (c.smem > (size_t)ctx.smem_optin) continue;
@@ -533,7 +533,8 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
           if (err == cudaSuccess) {
             char vb[96];
             std::snprintf(vb, sizeof vb, "thomas-pcr:tmem P2 S16 R%d x%d/%d%s%s", mc.R,
-                          mc.stages, mc.xstages, mc.w2s ? " w2s" : "",
+                          mc.stages, mc.xstages,
+                          mc.fmode == 2 ? " fbuf" : mc.fmode == 1 ? " w2s" : "",
                           contig ? " contig" : "");
             record(ctx, dir, "thomas-pcr", vb);
             return PENTAD_STATUS_SUCCESS;
@@ -643,7 +644,7 @@ struct Plan {
   int n_jobs = 0, total_tiles = 0, ctas = 0;
   struct Group {  // one batched launch: jobs [first, first + count) of the table
     int first, count, tiles;
-    bool w2s;
+    int fmode;  // factor mode of its grids
   };
   std::vector<Group> groups;
   std::vector<PlanSingle> singles;
@@ -685,12 +686,12 @@ pentadStatus_t plan_layout(Context &ctx, int count, const pentadsolver_grid_t *g
       *why = "an array pointer is null";
       return PENTAD_STATUS_INVALID_VALUE;
     }
-    bool w = false;
+    int w = 0;
     bool aligned = true;
     const void *ptrs[6] = {g.ds, g.dl, g.d, g.du, g.dw, g.x};
     for (const void *p : ptrs) aligned = aligned && reinterpret_cast<uintptr_t>(p) % sizeof(F) == 0;
     ok[i] = aligned && !env_flag("PENTA_NO_TMA") && tmem_shape<F>(shapes[i].L, contig, w);
-    need_w2s[i] = w;
+    need_w2s[i] = (char)w;
   }
   (void)ctx;
   w2s = false;
@@ -698,10 +699,10 @@ pentadStatus_t plan_layout(Context &ctx, int count, const pentadsolver_grid_t *g
   for (int i = 0; i < count; ++i)
     if (ok[i]) {
       order.push_back(i);
-      w2s = w2s || need_w2s[i];
+      w2s = w2s || need_w2s[i] != 0;
     }
-  // two job groups, one per factor mode (du2 and dw2 in TMEM; du2 alone),
-  // each heaviest lines first
+  // one job group per factor mode (du2 and dw2 in TMEM; du2 alone; all in
+  // the buffer), each heaviest lines first
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
     if (need_w2s[a] != need_w2s[b]) return need_w2s[a] < need_w2s[b];
     return shapes[a].L.n > shapes[b].L.n;
@@ -781,14 +782,14 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
       while (last < order.size() && gw2s[order[last]] == gw2s[order[first]]) ++last;
       int tiles = 0;
       if (!tmem_fill_jobs<F>(args.data() + first, (int)(last - first), contig,
-                             gw2s[order[first]] != 0, base,
+                             (int)gw2s[order[first]], base,
                              static_cast<unsigned char *>(host) + first * jb,
                              job_offs.data() + first, &tiles)) {
         std::free(host);
         *why = "tensor map encoding failed";
         return PENTAD_STATUS_INTERNAL_ERROR;
       }
-      groups.push_back({(int)first, (int)(last - first), tiles, gw2s[order[first]] != 0});
+      groups.push_back({(int)first, (int)(last - first), tiles, (int)gw2s[order[first]]});
       total_tiles += tiles;
       first = last;
     }
@@ -830,7 +831,7 @@ template <typename F> pentadStatus_t plan_run(Plan &p, cudaStream_t stream) {
   for (const Plan::Group &g : p.groups) {
     const cudaError_t e =
         launch_tmem_batch<F>(p.table + g.first * tmem_job_bytes<F>(), g.count, g.tiles,
-                             p.contig, g.w2s, p.discard, p.ctas, status, stream);
+                             p.contig, g.fmode, p.discard, p.ctas, status, stream);
     if (e != cudaSuccess) {
       cudaGetLastError();
       return PENTAD_STATUS_EXECUTION_FAILED;

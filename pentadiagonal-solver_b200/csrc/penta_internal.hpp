@@ -80,7 +80,7 @@ template <typename F> inline size_t tma_contig_scratch_bytes(const Lines &L) {
 // many grids of one direction and precision in one batched launch.
 struct TmemConfig {
   bool contig;   // along x (rows contiguous) or strided
-  bool w2s;      // dw2 in the buffer (longer lines), du2 alone in TMEM
+  int fmode;     // factors in TMEM: 0 du2 and dw2, 1 du2 (dw2 in the buffer), 2 none
   int stages;    // forward ring stages per consumer warp
   int xstages;   // read-back stages per consumer warp
   int R;         // rows per stage
@@ -88,11 +88,11 @@ struct TmemConfig {
 };
 template <typename F> const std::vector<TmemConfig> &tmem_configs();
 template <typename F> int tmem_occupancy(const TmemConfig &c);
-// A line set the kernel takes; `w2s` tells which factor mode it needs.
-template <typename F> bool tmem_shape(const Lines &L, bool contig, bool &w2s);
-template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig, bool w2s);
+// A line set the kernel takes; `fmode` tells which factor mode it needs.
+template <typename F> bool tmem_shape(const Lines &L, bool contig, int &fmode);
+template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig, int fmode);
 template <typename F>
-bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf, bool &w2s);
+bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf, int &fmode);
 template <typename F>
 cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count,
                         cudaStream_t stream);
@@ -101,12 +101,12 @@ cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count
 // device_base + scratch_offsets[i] (128-byte aligned for L2 discards).
 template <typename F> size_t tmem_job_bytes();
 template <typename F>
-bool tmem_fill_jobs(const SolveArgs<F> *grids, int count, bool contig, bool w2s,
+bool tmem_fill_jobs(const SolveArgs<F> *grids, int count, bool contig, int fmode,
                     unsigned char *device_base, void *host_jobs, size_t *scratch_offsets,
                     int *total_tiles);
 template <typename F>
 cudaError_t launch_tmem_batch(const void *device_jobs, int n_jobs, int total_tiles, bool contig,
-                              bool w2s, bool discard, int sm_count, int *status,
+                              int fmode, bool discard, int sm_count, int *status,
                               cudaStream_t stream);
 
 // shared_fact_kernels.cu: shared factorisation (line 0's coefficients for

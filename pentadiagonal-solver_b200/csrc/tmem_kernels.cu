@@ -27,25 +27,29 @@
 //    a stage into registers and releases the slot at once.
 //  * Factors in Tensor Memory (lanes 32c..32c+31, the quarter these warps can
 //    reach), one tcgen05.st per stage on the way down and one tcgen05.ld per
-//    stage on the way back:
-//      - du2 and dw2 (W2S = false): 4 columns per FP64 row, 2 per FP32 row;
+//    stage on the way back, in one of three factor modes FM:
+//      - 0, du2 and dw2 in TMEM: 4 columns per FP64 row, 2 per FP32 row;
 //        512 columns hold m <= 128 (FP64) / 256 (FP32) rows, n <= 256 / 512;
-//      - du2 only (W2S = true): half the columns, n <= 512 / 1024, with dw2
-//        travelling with x2 through the caller's buffer.
+//      - 1, du2 only: half the columns, n <= 512 / 1024, with dw2 travelling
+//        with x2 through the caller's buffer;
+//      - 2, none (longer lines): du2, dw2 and x2 all travel through the
+//        buffer, and n is bounded only by the buffer.
 //    Consecutive tiles of a warp fill TMEM blocks in opposite orders, so the
 //    blocks the back substitution of tile t frees first are the ones the
 //    forward sweep of tile t + 1 fills first; a progress word in shared
 //    memory (tile, steps done) tells the eliminating warp when a block is
 //    free.  The carries of the two halves are handed over in shared memory
 //    behind an mbarrier.
-//  * x2 (and dw2 when W2S) make an L2 round trip through the caller's buffer
-//    ([tile][half][m][16] of x2 or (dw2, x2) pairs), written once per row and
-//    read back, most recent first, by two bulk copies per stage into a small
-//    ring; each 128-byte line is dropped from L2 (discard.global.L2) once read,
-//    so it never reaches HBM.  The stores carry an evict-last L2 policy and
-//    the streamed accesses (coefficient and right-hand-side loads -- along x
-//    with dw2 in the buffer excepted --, results, read-backs) an evict-first
-//    one, so that the scratch survives in L2 while the arrays stream past it.
+//  * x2 (and dw2, du2 as the mode has it) make an L2 round trip through the
+//    caller's buffer ([tile][half][m][16] of x2, [..][16][2] (dw2, x2) pairs,
+//    or [..][m][3][16] with du2, dw2, x2 each a 128-byte line per row),
+//    written once per row and read back, most recent first, by two bulk
+//    copies per stage into a small ring; each 128-byte line is dropped from
+//    L2 (discard.global.L2) once read, so it never reaches HBM while it fits
+//    in L2.  The stores carry an evict-last L2 policy and the streamed
+//    accesses (coefficient and right-hand-side loads -- along x with factors
+//    in the buffer excepted --, results, read-backs) an evict-first one, so
+//    that the scratch survives in L2 while the arrays stream past it.
 //  * Output: strided directions store x directly (16 consecutive lines are one
 //    128-byte segment).  Along x, a lane's rows are contiguous in memory: the
 //    results of two steps go into a 128-byte-swizzled shared tile of 2R rows
@@ -102,19 +106,19 @@ template <typename F, bool CONTIG> constexpr int tmem_rows_per_stage() {
   return CONTIG ? 64 / (int)sizeof(F) : 1024 / (TS * (int)sizeof(F));
 }
 // TMEM columns per stage: R rows of du2, dw2 (or du2 alone), sizeof(F)/4 each.
-template <typename F, bool W2S> constexpr int tmem_cols_per_stage() {
-  return 64 / (int)sizeof(F) * (W2S ? 1 : 2) * (int)sizeof(F) / 4;
+template <typename F, int FM> constexpr int tmem_cols_per_stage() {
+  return 64 / (int)sizeof(F) * (FM == 0 ? 2 : 1) * (int)sizeof(F) / 4;
 }
 
-template <typename F, bool CONTIG, bool W2S, int ST, int XST> struct TmemGeom {
+template <typename F, bool CONTIG, int FM, int ST, int XST> struct TmemGeom {
   static constexpr int R = tmem_rows_per_stage<F, CONTIG>();
-  static constexpr int PW = W2S ? 2 : 1;              // scratch values per row
+  static constexpr int PW = FM == 2 ? 3 : (FM == 1 ? 2 : 1);  // scratch values per row
   static constexpr int BOX = R * TS;                  // elements per TMA tile
   static constexpr int SE = 12 * BOX;                 // forward stage
   static constexpr int XE = 2 * R * TS * PW;          // read-back stage
   static constexpr int OBE = CONTIG ? 8 * BOX : 0;    // output: 2 buffers x 2 halves x 2R rows
   static constexpr int HE = 2 * 6 * 32;               // carries: 2 slots x 6 values x 32 lanes
-  static constexpr int kCols = tmem_cols_per_stage<F, W2S>();
+  static constexpr int kCols = tmem_cols_per_stage<F, FM>();
   static constexpr int NB = (int)kTmemCols / kCols;   // TMEM blocks of one stage each
   static constexpr size_t kData = (size_t)(ST * SE + XST * XE + OBE + HE) * sizeof(F);
   static constexpr size_t kBars = (size_t)(2 * ST + XST + 2) * 8;
@@ -124,7 +128,7 @@ template <typename F, bool CONTIG, bool W2S, int ST, int XST> struct TmemGeom {
   // at least 116 KB, so that one CTA holds an SM (and all of its TMEM)
   static constexpr size_t kSmem = kUsed > 118784 ? kUsed : 118784;
   static_assert(kSmem <= 232448, "shared memory per CTA");
-  static_assert(R * (W2S ? 1 : 2) * (int)sizeof(F) / 4 == kCols, "TMEM columns per stage");
+  static_assert(R * (FM == 0 ? 2 : 1) * (int)sizeof(F) / 4 == kCols, "TMEM columns per stage");
 };
 
 template <typename F> __device__ __forceinline__ void put_bits(uint32_t *tv, int c, F v);
@@ -143,11 +147,11 @@ template <> __device__ __forceinline__ float get_bits<float>(const uint32_t *tv,
   return __uint_as_float(tv[c]);
 }
 
-template <typename F, bool CONTIG, bool W2S, int ST, int XST, bool BATCH>
+template <typename F, bool CONTIG, int FM, int ST, int XST, bool BATCH>
 __global__ void __launch_bounds__(96 * NCONS, 1)
 tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__restrict__ jobs,
                    int n_jobs, int total_tiles, int flags, int *__restrict__ status_word) {
-  using G = TmemGeom<F, CONTIG, W2S, ST, XST>;
+  using G = TmemGeom<F, CONTIG, FM, ST, XST>;
   using V2 = typename Vec2<F>::T;
   constexpr int R = G::R, BOX = G::BOX, SE = G::SE, XE = G::XE, PW = G::PW, NB = G::NB;
   constexpr int EPC = 16 / (int)sizeof(F);  // elements per 16-byte chunk
@@ -238,7 +242,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   if (role == 1) {
     // read once: evict first -- except along x with dw2 in the buffer, where
     // the larger scratch round trip does better against normal-priority loads
-    const uint64_t pol_in = (CONTIG && W2S) ? l2_policy_normal() : l2_policy_first();
+    const uint64_t pol_in = (CONTIG && FM >= 1) ? l2_policy_normal() : l2_policy_first();
     int slot = 0, use = 0, cursor = 0, fenced = -1;
     Geo JG;
     load_geo(job_of(gw, cursor), JG);
@@ -400,7 +404,10 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
       const int n_stages = mt / R;
       const int nvp = part ? 2 * mt - n : 0;  // this half's virtual rows
       const int count = CONTIG ? min(TS, JG.n_sys - c0) : min(TS, JG.inner - c0);
-      F *const x2w = JG.scratch + (long long)tile * 2 * mt * TS * PW + (part * mt * TS + sys) * PW;
+      // this lane's scratch: row k at + k 16 PW (all factors: component c of
+      // row k at + (3 k + c) 16, so that each component is one 128-byte line)
+      F *const x2w = JG.scratch + (long long)tile * 2 * mt * TS * PW +
+                     (FM == 2 ? part * mt * TS * PW + sys : (part * mt * TS + sys) * PW);
       const bool flip = (ti & 1) != 0;
       const int free_blocks = NB - n_prev;  // blocks the previous tile never used
       Carry<F> c;
@@ -452,11 +459,12 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         for (int r = 0; r < R; ++r)
           fwd_row_lean(a[r][0], a[r][1], a[r][2], a[r][3], a[r][4], a[r][5], c, u[r], w[r],
                        y[r]);
+        if constexpr (FM < 2) {  // du2 (and dw2) into TMEM
         uint32_t tv[G::kCols];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          put_bits<F>(tv, r * CW * (W2S ? 1 : 2), u[r]);
-          if (!W2S) put_bits<F>(tv, r * CW * 2 + CW, w[r]);
+          put_bits<F>(tv, r * CW * (FM == 0 ? 2 : 1), u[r]);
+          if (FM == 0) put_bits<F>(tv, r * CW * 2 + CW, w[r]);
         }
         // wait (lane 0, bounded) until the previous tile has read this block
         const int need = (ti - 1) * 65536 + max(0, g + 1 - free_blocks);
@@ -491,10 +499,15 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
           tmem_store32(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[32]>(tv));
         else
           tmem_store16(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[16]>(tv));
+        }
         F *const x2g = x2w + g * R * TS * PW;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          if constexpr (W2S) {
+          if constexpr (FM == 2) {
+            st_hint(x2g + (3 * r) * TS, u[r], pol_x2);
+            st_hint(x2g + (3 * r + 1) * TS, w[r], pol_x2);
+            st_hint(x2g + (3 * r + 2) * TS, y[r], pol_x2);
+          } else if constexpr (FM == 1) {
             V2 pv;
             pv.x = w[r];
             pv.y = y[r];
@@ -650,24 +663,31 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         const int g = n_stages - 1 - s;  // the forward stage being undone
         const int blk = flip ? NB - 1 - g : g;
         uint32_t tv[G::kCols];
-        if constexpr (G::kCols == 32)
-          tmem_load32(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[32]>(tv));
-        else
-          tmem_load16(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[16]>(tv));
-        // the block is free for the next tile's forward sweep
-        tmem_fence_before_sync();
-        __syncwarp();
-        if (lane == 0) st_release_shared(&prog[cons], ti * 65536 + s + 1);
+        if constexpr (FM < 2) {
+          if constexpr (G::kCols == 32)
+            tmem_load32(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[32]>(tv));
+          else
+            tmem_load16(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[16]>(tv));
+          // the block is free for the next tile's forward sweep
+          tmem_fence_before_sync();
+          __syncwarp();
+          if (lane == 0) st_release_shared(&prog[cons], ti * 65536 + s + 1);
+        }
         if (!__all_sync(0xffffffffu, mbar_wait(&rfull[r_slot], r_phase))) {
           fail = 1;
           break;
         }
-        const F *xsrc = xr + r_slot * XE + (part * R * TS + sys) * PW;
+        const F *xsrc = xr + r_slot * XE +
+                        (FM == 2 ? part * R * TS * PW + sys : (part * R * TS + sys) * PW);
         F xs[R], du[R], dw[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int j = R - 1 - r;  // row inside the stage block
-          if constexpr (W2S) {
+          if constexpr (FM == 2) {
+            du[r] = xsrc[(3 * j) * TS];
+            dw[r] = xsrc[(3 * j + 1) * TS];
+            xs[r] = xsrc[(3 * j + 2) * TS];
+          } else if constexpr (FM == 1) {
             const V2 pv = *reinterpret_cast<const V2 *>(xsrc + j * TS * 2);
             dw[r] = pv.x;
             xs[r] = pv.y;
@@ -689,10 +709,10 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         }
         // the stage's block of each half is dead: drop its 128-byte lines
         constexpr int kLines = (int)(kBlock / 128);
-        if (drop && sys < kLines)
+        for (int l = sys; drop && l < kLines; l += TS)
           discard_l2_line(reinterpret_cast<const unsigned char *>(
                               x2t + (long long)(part * mt + mt - (s + 1) * R) * TS * PW) +
-                          sys * 128);
+                          l * 128);
         F xk[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -830,17 +850,16 @@ long long tile_count(const Lines &L, bool contig) {
 // Is this line set one the kernel takes (apart from the buffer)?  Also gives
 // whether it needs the dw2-in-buffer mode.
 template <typename F>
-bool shape_ok(const Lines &L, bool contig, bool &w2s) {
+bool shape_ok(const Lines &L, bool contig, int &fmode) {
   if (contig ? L.inner != 1 : L.inner <= 1) return false;
   const long long R =
       contig ? tmem_rows_per_stage<F, true>() : tmem_rows_per_stage<F, false>();
   const long long mt = split_row<F>(L, contig);
   if (L.n - mt < 2) return false;  // two real rows per half
   const long long stages = mt / R;
-  const long long cap_both = kTmemCols / tmem_cols_per_stage<F, false>();
-  const long long cap_du = kTmemCols / tmem_cols_per_stage<F, true>();
-  if (stages > cap_du) return false;
-  w2s = stages > cap_both;
+  const long long cap_both = kTmemCols / tmem_cols_per_stage<F, 0>();
+  const long long cap_du = kTmemCols / tmem_cols_per_stage<F, 1>();
+  fmode = stages > cap_du ? 2 : stages > cap_both ? 1 : 0;
   if (L.n * L.n_sys >= (1LL << 31) || tile_count(L, contig) >= (1LL << 31)) return false;
   return true;
 }
@@ -855,9 +874,9 @@ template <typename F> bool tma_ok(const SolveArgs<F> &a, bool contig) {
   return true;
 }
 
-template <typename F> size_t job_scratch_bytes(const Lines &L, bool contig, bool w2s) {
+template <typename F> size_t job_scratch_bytes(const Lines &L, bool contig, int fmode) {
   return (size_t)tile_count(L, contig) * 2 * (size_t)split_row<F>(L, contig) * TS *
-         (w2s ? 2 : 1) * sizeof(F);
+         (fmode == 2 ? 3 : fmode == 1 ? 2 : 1) * sizeof(F);
 }
 
 template <typename F>
@@ -883,12 +902,12 @@ bool fill_job(TmemJob<F> &J, const SolveArgs<F> &a, bool contig, F *scratch, int
   return true;
 }
 
-template <typename F, bool CONTIG, bool W2S, int ST, int XST, bool BATCH>
+template <typename F, bool CONTIG, int FM, int ST, int XST, bool BATCH>
 cudaError_t tmem_launch_raw(const TmemJob<F> &job1, const TmemJob<F> *jobs, int n_jobs,
                             int total_tiles, int flags, int sm_count, int *status,
                             cudaStream_t stream) {
-  using G = TmemGeom<F, CONTIG, W2S, ST, XST>;
-  auto kern = tmem_thomas_kernel<F, CONTIG, W2S, ST, XST, BATCH>;
+  using G = TmemGeom<F, CONTIG, FM, ST, XST>;
+  auto kern = tmem_thomas_kernel<F, CONTIG, FM, ST, XST, BATCH>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)G::kSmem);
   if (err != cudaSuccess) return err;
@@ -899,9 +918,9 @@ cudaError_t tmem_launch_raw(const TmemJob<F> &job1, const TmemJob<F> *jobs, int 
   return cudaGetLastError();
 }
 
-template <typename F, bool CONTIG, bool W2S, int ST, int XST> int tmem_occ() {
-  using G = TmemGeom<F, CONTIG, W2S, ST, XST>;
-  auto kern = tmem_thomas_kernel<F, CONTIG, W2S, ST, XST, false>;
+template <typename F, bool CONTIG, int FM, int ST, int XST> int tmem_occ() {
+  using G = TmemGeom<F, CONTIG, FM, ST, XST>;
+  auto kern = tmem_thomas_kernel<F, CONTIG, FM, ST, XST, false>;
   int blocks = 0;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)G::kSmem) != cudaSuccess ||
@@ -920,23 +939,27 @@ template <typename F, bool CONTIG, bool W2S, int ST, int XST> int tmem_occ() {
 // launches use the default variants.  Along x two forward stages beat three:
 // fewer 64-byte requests in flight per line keep HBM row hits up (measured at
 // 256^3 and 512^3); the strided directions want three.
-#define PENTA_TMEM_CONFIGS(X)   \
-  X(double, true, false, 2, 4)  \
-  X(double, true, false, 3, 4)  \
-  X(double, true, false, 3, 3)  \
-  X(double, false, false, 3, 4) \
-  X(double, false, false, 3, 3) \
-  X(double, false, false, 2, 4) \
-  X(double, true, true, 2, 3)   \
-  X(double, true, true, 3, 2)   \
-  X(double, false, true, 3, 4)  \
-  X(float, true, false, 2, 4)   \
-  X(float, true, false, 3, 4)   \
-  X(float, false, false, 3, 4)  \
-  X(float, false, false, 4, 3)  \
-  X(float, true, true, 2, 3)    \
-  X(float, true, true, 3, 2)    \
-  X(float, false, true, 3, 4)
+#define PENTA_TMEM_CONFIGS(X) \
+  X(double, true, 0, 2, 4)    \
+  X(double, true, 0, 3, 4)    \
+  X(double, true, 0, 3, 3)    \
+  X(double, false, 0, 3, 4)   \
+  X(double, false, 0, 3, 3)   \
+  X(double, false, 0, 2, 4)   \
+  X(double, true, 1, 2, 3)    \
+  X(double, true, 1, 3, 2)    \
+  X(double, false, 1, 3, 4)   \
+  X(double, true, 2, 2, 2)    \
+  X(double, false, 2, 3, 2)   \
+  X(float, true, 0, 2, 4)     \
+  X(float, true, 0, 3, 4)     \
+  X(float, false, 0, 3, 4)    \
+  X(float, false, 0, 4, 3)    \
+  X(float, true, 1, 2, 3)     \
+  X(float, true, 1, 3, 2)     \
+  X(float, false, 1, 3, 4)    \
+  X(float, true, 2, 2, 2)     \
+  X(float, false, 2, 3, 2)
 
 template <typename F> const std::vector<TmemConfig> &tmem_configs() {
   static const std::vector<TmemConfig> v = [] {
@@ -954,7 +977,7 @@ template <typename F> const std::vector<TmemConfig> &tmem_configs() {
 
 template <typename F> int tmem_occupancy(const TmemConfig &c) {
 #define PENTA_X(FT_, C_, W_, ST_, XST_)                                                  \
-  if (std::is_same<F, FT_>::value && c.contig == C_ && c.w2s == W_ && c.stages == ST_ && \
+  if (std::is_same<F, FT_>::value && c.contig == C_ && c.fmode == W_ && c.stages == ST_ && \
       c.xstages == XST_)                                                                 \
     return tmem_occ<FT_, C_, W_, ST_, XST_>();
   PENTA_TMEM_CONFIGS(PENTA_X)
@@ -962,19 +985,19 @@ template <typename F> int tmem_occupancy(const TmemConfig &c) {
   return 0;
 }
 
-template <typename F> bool tmem_shape(const Lines &L, bool contig, bool &w2s) {
-  return shape_ok<F>(L, contig, w2s);
+template <typename F> bool tmem_shape(const Lines &L, bool contig, int &fmode) {
+  return shape_ok<F>(L, contig, fmode);
 }
 
-template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig, bool w2s) {
-  return job_scratch_bytes<F>(L, contig, w2s);
+template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig, int fmode) {
+  return job_scratch_bytes<F>(L, contig, fmode);
 }
 
 template <typename F>
-bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf, bool &w2s) {
-  if (!tmem_shape<F>(a.L, contig, w2s)) return false;
+bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf, int &fmode) {
+  if (!tmem_shape<F>(a.L, contig, fmode)) return false;
   if (a.scratch == nullptr || reinterpret_cast<uintptr_t>(a.scratch) % 16 != 0 ||
-      tmem_scratch_bytes<F>(a.L, contig, w2s) > usable_buf)
+      tmem_scratch_bytes<F>(a.L, contig, fmode) > usable_buf)
     return false;
   const void *ptrs[6] = {a.ds, a.dl, a.d, a.du, a.dw, a.x};
   for (const void *p : ptrs)  // element alignment (TMA needs 16 bytes; see tma_ok)
@@ -990,7 +1013,7 @@ cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count
     return cudaErrorInvalidValue;
   const int flags = ((reinterpret_cast<uintptr_t>(a.scratch) % 128 == 0) ? 1 : 0);
 #define PENTA_X(FT_, C_, W_, ST_, XST_)                                                   \
-  if (std::is_same<F, FT_>::value && c.contig == C_ && c.w2s == W_ && c.stages == ST_ &&  \
+  if (std::is_same<F, FT_>::value && c.contig == C_ && c.fmode == W_ && c.stages == ST_ &&  \
       c.xstages == XST_)                                                                  \
     return tmem_launch_raw<FT_, C_, W_, ST_, XST_, false>(                                \
         reinterpret_cast<const TmemJob<FT_> &>(J), nullptr, 1, J.n_tiles, flags, sm_count, \
@@ -1004,7 +1027,7 @@ cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count
 template <typename F> size_t tmem_job_bytes() { return sizeof(TmemJob<F>); }
 
 template <typename F>
-bool tmem_fill_jobs(const SolveArgs<F> *grids, int count, bool contig, bool w2s,
+bool tmem_fill_jobs(const SolveArgs<F> *grids, int count, bool contig, int fmode,
                     unsigned char *device_base, void *host_jobs, size_t *scratch_offsets,
                     int *total_tiles) {
   TmemJob<F> *J = static_cast<TmemJob<F> *>(host_jobs);
@@ -1015,54 +1038,60 @@ bool tmem_fill_jobs(const SolveArgs<F> *grids, int count, bool contig, bool w2s,
     tiles += J[i].n_tiles;
   }
   *total_tiles = tiles;
-  (void)w2s;
+  (void)fmode;
   return true;
 }
 
 template <typename F>
 cudaError_t launch_tmem_batch(const void *device_jobs, int n_jobs, int total_tiles, bool contig,
-                              bool w2s, bool discard, int sm_count, int *status,
+                              int fmode, bool discard, int sm_count, int *status,
                               cudaStream_t stream) {
   TmemJob<F> none;
   std::memset(&none, 0, sizeof(none));
   const TmemJob<F> *jobs = static_cast<const TmemJob<F> *>(device_jobs);
   const int flags = discard ? 1 : 0;
-  if (contig && !w2s)
-    return tmem_launch_raw<F, true, false, 2, 4, true>(none, jobs, n_jobs, total_tiles, flags,
-                                                       sm_count, status, stream);
-  if (contig && w2s)
-    return tmem_launch_raw<F, true, true, 2, 3, true>(none, jobs, n_jobs, total_tiles, flags,
-                                                      sm_count, status, stream);
-  if (!w2s)
-    return tmem_launch_raw<F, false, false, 3, 4, true>(none, jobs, n_jobs, total_tiles, flags,
-                                                        sm_count, status, stream);
-  return tmem_launch_raw<F, false, true, 3, 4, true>(none, jobs, n_jobs, total_tiles, flags,
-                                                     sm_count, status, stream);
+  if (contig && fmode == 0)
+    return tmem_launch_raw<F, true, 0, 2, 4, true>(none, jobs, n_jobs, total_tiles, flags,
+                                                   sm_count, status, stream);
+  if (contig && fmode == 1)
+    return tmem_launch_raw<F, true, 1, 2, 3, true>(none, jobs, n_jobs, total_tiles, flags,
+                                                   sm_count, status, stream);
+  if (contig)
+    return tmem_launch_raw<F, true, 2, 2, 2, true>(none, jobs, n_jobs, total_tiles, flags,
+                                                   sm_count, status, stream);
+  if (fmode == 0)
+    return tmem_launch_raw<F, false, 0, 3, 4, true>(none, jobs, n_jobs, total_tiles, flags,
+                                                    sm_count, status, stream);
+  if (fmode == 1)
+    return tmem_launch_raw<F, false, 1, 3, 4, true>(none, jobs, n_jobs, total_tiles, flags,
+                                                    sm_count, status, stream);
+  return tmem_launch_raw<F, false, 2, 3, 2, true>(none, jobs, n_jobs, total_tiles, flags,
+                                                  sm_count, status, stream);
 }
 
 template const std::vector<TmemConfig> &tmem_configs<double>();
 template const std::vector<TmemConfig> &tmem_configs<float>();
 template int tmem_occupancy<double>(const TmemConfig &);
 template int tmem_occupancy<float>(const TmemConfig &);
-template bool tmem_shape<double>(const Lines &, bool, bool &);
-template bool tmem_shape<float>(const Lines &, bool, bool &);
-template size_t tmem_scratch_bytes<double>(const Lines &, bool, bool);
-template size_t tmem_scratch_bytes<float>(const Lines &, bool, bool);
-template bool tmem_supported<double>(const SolveArgs<double> &, bool, size_t, bool &);
-template bool tmem_supported<float>(const SolveArgs<float> &, bool, size_t, bool &);
+template bool tmem_shape<double>(const Lines &, bool, int &);
+template bool tmem_shape<float>(const Lines &, bool, int &);
+template size_t tmem_scratch_bytes<double>(const Lines &, bool, int);
+template size_t tmem_scratch_bytes<float>(const Lines &, bool, int);
+template bool tmem_supported<double>(const SolveArgs<double> &, bool, size_t, int &);
+template bool tmem_supported<float>(const SolveArgs<float> &, bool, size_t, int &);
 template cudaError_t launch_tmem<double>(const SolveArgs<double> &, const TmemConfig &, int,
                                          cudaStream_t);
 template cudaError_t launch_tmem<float>(const SolveArgs<float> &, const TmemConfig &, int,
                                         cudaStream_t);
 template size_t tmem_job_bytes<double>();
 template size_t tmem_job_bytes<float>();
-template bool tmem_fill_jobs<double>(const SolveArgs<double> *, int, bool, bool, unsigned char *,
+template bool tmem_fill_jobs<double>(const SolveArgs<double> *, int, bool, int, unsigned char *,
                                      void *, size_t *, int *);
-template bool tmem_fill_jobs<float>(const SolveArgs<float> *, int, bool, bool, unsigned char *,
+template bool tmem_fill_jobs<float>(const SolveArgs<float> *, int, bool, int, unsigned char *,
                                     void *, size_t *, int *);
-template cudaError_t launch_tmem_batch<double>(const void *, int, int, bool, bool, bool, int,
+template cudaError_t launch_tmem_batch<double>(const void *, int, int, bool, int, bool, int,
                                                int *, cudaStream_t);
-template cudaError_t launch_tmem_batch<float>(const void *, int, int, bool, bool, bool, int,
+template cudaError_t launch_tmem_batch<float>(const void *, int, int, bool, int, bool, int,
                                               int *, cudaStream_t);
 
 }  // namespace penta

@@ -259,10 +259,11 @@ def test_256cube_properties(cuda, solvedim):
 
 def _tmem_ok(dims, solvedim, eb):
     """Shapes the Tensor-Memory kernel takes (TMA tiles when rows (x) or runs
-    (y, z) are 16-byte aligned, element copies otherwise): two real rows in each half of the split m = R ceil(n / 2R), m / R
-    stages within 512 TMEM columns (du2 and dw2 there: 16 stages; du2 alone,
-    dw2 in the buffer: 32 stages), and its scratch for whole tiles of 16 lines
-    within the reference-sized buffer."""
+    (y, z) are 16-byte aligned, element copies otherwise): two real rows in
+    each half of the split m = R ceil(n / 2R), and its scratch for whole tiles
+    of 16 lines within the reference-sized buffer.  The factor mode follows
+    the m / R stages: du2 and dw2 in 512 TMEM columns (16 stages), du2 alone
+    with dw2 in the buffer (32 stages), or all factors in the buffer."""
     n = dims[solvedim]
     inner = int(np.prod(dims[:solvedim]))
     n_sys = int(np.prod(dims)) // n
@@ -272,11 +273,11 @@ def _tmem_ok(dims, solvedim, eb):
     mt = r * (-(-n // (2 * r)))
     stages = mt // r
     cols = r * eb // 4               # TMEM columns of one factor per stage
-    w2s = stages > 512 // (2 * cols)
+    per_row = 1 if stages <= 512 // (2 * cols) else 2 if stages <= 512 // cols else 3
     tiles = -(-n_sys // 16) if contig else (n_sys // inner) * -(-inner // 16)
-    need = tiles * 2 * mt * 16 * eb * (2 if w2s else 1)
+    need = tiles * 2 * mt * 16 * eb * per_row
     buf = ps.buffer_size(list(dims), solvedim, eb)
-    return aligned and n - mt >= 2 and stages <= 512 // cols and need <= buf
+    return aligned and n - mt >= 2 and need <= buf
 
 
 def _old_tma_ok(dims, solvedim, eb, buffer=True):
@@ -354,3 +355,28 @@ def test_kernel_chain_every_direction(cuda, dims, dtype, monkeypatch):
         assert "tmem" not in v and ("tma" in v) == (old and solvedim != 0), (solvedim, v)
         v = check((), buffer=False)
         assert "tmem" not in v, (solvedim, v)
+
+
+LONG_DIMS = [((1040, 16, 5), 0), ((16, 1104, 5), 1), ((16, 5, 1040), 2), ((1033, 16, 5), 0),
+             ((2100, 16, 5), 0), ((16, 2048, 5), 1), ((40, 1100, 5), 1)]
+
+
+@pytest.mark.parametrize("dims,solvedim", LONG_DIMS)
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_long_lines_factors_in_the_buffer(cuda, dims, solvedim, dtype):
+    """Lines longer than Tensor Memory holds (n > 512 FP64 / 1024 FP32): the
+    Tensor-Memory kernel keeps all factors in the buffer (variant "fbuf")
+    and agrees with the oracle; odd n along x takes its element copies."""
+    eb = np.dtype(dtype).itemsize
+    co = fixtures.random_dominant(dims, 500 + solvedim, dtype)
+    ref = {k: co[k].astype(np.float64) for k in NAMES}
+    oracle.solve(ref["ds"], ref["dl"], ref["d"], ref["du"], ref["dw"], ref["x"], solvedim)
+    dv = to_dev(co)
+    with ps.Handle() as h:
+        solve_dev(dv, solvedim, handle=h)
+        var = h.variant_that_ran(direction(len(dims), solvedim))
+    assert fwd_err(dv["x"].cpu().numpy(), ref["x"]) <= FWD_TOL[dtype], (dims, var)
+    n = dims[solvedim]
+    long_line = n > (512 if eb == 8 else 1024)
+    if _tmem_ok(dims, solvedim, eb):
+        assert "tmem" in var and (("fbuf" in var) == long_line), (dims, var)

@@ -36,7 +36,8 @@ def oracle_solution(co, solvedim):
 def test_plan_uneven_grids_match_oracle(cuda, dtype, solvedim):
     # odd and even extents, lines of 5 (solved alone: too short for the halves
     # of the batched kernel), and long lines (du2-only factor mode)
-    extra = [(300, 6, 5), (6, 290, 5), (5, 5, 260), (5, 5, 5), (64, 64, 64)]
+    extra = [(300, 6, 5), (6, 290, 5), (5, 5, 260), (5, 5, 5), (64, 64, 64), (1040, 16, 5),
+             (5, 16, 1100)]
     dims_list = uneven_dims(14, 100 + solvedim, extra=extra)
     probs = [fixtures.random_dominant(dims, 40 + i, dtype) for i, dims in enumerate(dims_list)]
     refs = [oracle_solution(co, solvedim) for co in probs]
