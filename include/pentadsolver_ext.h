@@ -76,9 +76,10 @@ EXTERN_C PENTAD_API const char *pentadsolver_status_string(pentadStatus_t status
  * mix of shapes, one precision, one solvedim) with one launch of the batched
  * Tensor-Memory kernel; grids that kernel does not take (lines too short or
  * too long) are solved one by one inside the same execute.  Creating a plan
- * writes its job table into the caller's buffer (a synchronous copy);
- * executing it launches kernels on `stream` only, so an execute can be
- * captured into a CUDA graph and replayed.  The grids' arrays and the buffer
+ * writes its job table into the caller's buffer with a copy that returns
+ * when done and waits for no other stream, so the buffer must not be in use
+ * by queued work; executing it launches kernels on `stream` only, so an
+ * execute can be captured into a CUDA graph and replayed.  The grids' arrays and the buffer
  * must stay valid and unmoved for the plan's lifetime; their contents may
  * change between executes (x is solved in place each time). */
 typedef struct pentadsolver_grid {

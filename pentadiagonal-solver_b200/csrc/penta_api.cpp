@@ -101,6 +101,7 @@ struct Context {
   std::string variant[3];
   std::string tuning[3];  // pentadsolver_set_tuning, per direction ("" = none)
   std::unordered_map<long long, int> occ_cache;  // (variant, n) -> CTAs/SM
+  cudaStream_t copy_stream = nullptr;  // non-blocking: plan-table uploads (copy_h2d)
 
   bool init() {  // idempotent; needs a usable device
     if (device >= 0) return true;
@@ -123,6 +124,25 @@ struct Context {
     return true;
   }
 };
+
+// Host -> device copy that waits only for itself: on the context's
+// non-blocking stream, so creating a plan never waits for solves that run on
+// other streams (a plain cudaMemcpy on the legacy stream can).
+cudaError_t copy_h2d(Context &ctx, void *dst, const void *src, size_t bytes) {
+  cudaStream_t s = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(ctx.mu);
+    if (ctx.copy_stream == nullptr &&
+        cudaStreamCreateWithFlags(&ctx.copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      ctx.copy_stream = nullptr;
+      return cudaGetLastError();
+    }
+    s = ctx.copy_stream;
+  }
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e;
+}
 
 std::mutex g_reg_mu;
 std::unordered_set<Context *> g_live;
@@ -793,7 +813,7 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
       total_tiles += tiles;
       first = last;
     }
-    const cudaError_t e = cudaMemcpy(table, host, order.size() * jb, cudaMemcpyHostToDevice);
+    const cudaError_t e = copy_h2d(ctx, table, host, order.size() * jb);
     std::free(host);
     if (e != cudaSuccess) {
       cudaGetLastError();
@@ -1469,7 +1489,7 @@ extern "C" pentadStatus_t pentadsolver_refine_plan_create(pentadsolver_handle_t 
     table[i].chunk_base = chunks;
     chunks += penta::refine_chunks(table[i].n_points);
   }
-  if (cudaMemcpy(base, table.data(), count * sizeof(penta::RefineGrid), cudaMemcpyHostToDevice) !=
+  if (penta::copy_h2d(*ctx, base, table.data(), count * sizeof(penta::RefineGrid)) !=
       cudaSuccess) {
     cudaGetLastError();
     delete fp32;

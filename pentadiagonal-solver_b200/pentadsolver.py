@@ -323,6 +323,10 @@ class Plan:
             off = (-self.buffer.data_ptr()) % 256
             self._buf = self.buffer[off:off + self.buffer_bytes]
         self._plan = _P(None)
+        # plan creation writes the job table into the new buffer without
+        # waiting for other streams: the allocator may have handed out memory
+        # that work queued on this stream still uses, so let that finish
+        idle = torch.cuda.current_stream(self.device).synchronize
         if scratch is not None and not self.refine:
             # job table in its own small buffer, scratch shared with other
             # plans that never run at the same time
@@ -333,6 +337,7 @@ class Plan:
             self.buffer = torch.empty(tb + 512, dtype=torch.uint8, device=self.device)
             off = (-self.buffer.data_ptr()) % 256
             self._buf = self.buffer[off:off + max(tb, 256)]
+            idle()
             st = _typed("pentadsolver_plan_create_split",
                         [_P, _I, _I, ctypes.POINTER(GridDesc), _I, _P, _Z, _P, _Z, _I,
                          ctypes.POINTER(_P)])(
@@ -342,6 +347,7 @@ class Plan:
             if st != SUCCESS:
                 raise PentadError(st, "plan create")
             return
+        idle()
         if self.refine:
             st = _typed("pentadsolver_refine_plan_create",
                         [_P, _I, ctypes.POINTER(GridDesc), _I, _I, _P, _Z, _I, ctypes.POINTER(_P)])(
