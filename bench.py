@@ -38,6 +38,7 @@ for p in (str(PKG), str(REPO)):
 
 N_DEFAULT = 256
 ITERS = 50
+EV_EVERY = 5  # iterations between timed launches (per-direction launch times)
 R_DIFF = 0.5
 SEED = 2024
 BYTES_PER_POINT_AXIS = 7 * 8
@@ -166,12 +167,13 @@ def run_ours(args):
 
     def step(x, dir_events=None):
         for it in range(ITERS):
+            timed_it = dir_events is not None and it % EV_EVERY == 0
             for axis in range(3):
-                if dir_events is not None:
-                    dir_events[it][axis][0].record(stream)
+                if timed_it:
+                    dir_events[it // EV_EVERY][axis][0].record(stream)
                 solve(axis, x)
-                if dir_events is not None:
-                    dir_events[it][axis][1].record(stream)
+                if timed_it:
+                    dir_events[it // EV_EVERY][axis][1].record(stream)
 
     x = d["x"]
     torch.cuda.synchronize()
@@ -185,10 +187,11 @@ def run_ours(args):
     # ---- timed region: K steps, device time ---------------------------------
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    # an event pair around every launch of the timed region (average launch
-    # duration per direction, for the roofline)
+    # an event pair around every launch of every EV_EVERY-th iteration of the
+    # timed region (average launch duration per direction, for the roofline;
+    # sampled so that the records add little to the step time)
     dir_ev = [[[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(3)]
-               for _ in range(ITERS)] for _ in range(args.steps)]
+               for _ in range(ITERS // EV_EVERY)] for _ in range(args.steps)]
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -206,8 +209,8 @@ def run_ours(args):
         ms_total = float(t.item())
         dist.barrier()
     ms_step = ms_total / args.steps
-    per_dir_ms = [statistics.mean(dir_ev[k][it][a][0].elapsed_time(dir_ev[k][it][a][1])
-                                  for k in range(args.steps) for it in range(ITERS))
+    per_dir_ms = [statistics.mean(dir_ev[k][j][a][0].elapsed_time(dir_ev[k][j][a][1])
+                                  for k in range(args.steps) for j in range(ITERS // EV_EVERY))
                   for a in range(3)]
     alg_bytes_step = BYTES_PER_POINT_AXIS * n ** 3 * 3 * ITERS
     value = world * alg_bytes_step / (ms_step * 1e-3) / 1e9
