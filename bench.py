@@ -39,6 +39,27 @@ for p in (str(PKG), str(REPO)):
 N_DEFAULT = 256
 ITERS = 50
 EV_EVERY = 5  # iterations between timed launches (per-direction launch times)
+
+
+def max_over_ranks(ms: float, world: int, device) -> float:
+    """The slowest rank's time, on every rank (replicas finish when the last
+    one does).  `device` holds the reduction tensor: the GPU under NCCL, the
+    CPU under gloo."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gbs(bytes_per_rank: float, ms: float, world: int) -> float:
+    """GB/s of all ranks together: every replica moves `bytes_per_rank` in `ms`."""
+    return world * bytes_per_rank / (ms * 1e-3) / 1e9
+
+
 R_DIFF = 0.5
 SEED = 2024
 BYTES_PER_POINT_AXIS = 7 * 8
@@ -203,17 +224,15 @@ def run_ours(args):
         stream.synchronize()
     torch.cuda.synchronize()
     ms_total = ev0.elapsed_time(ev1)
+    ms_total = max_over_ranks(ms_total, world, dev)
     if world > 1:
-        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
         dist.barrier()
     ms_step = ms_total / args.steps
     per_dir_ms = [statistics.mean(dir_ev[k][j][a][0].elapsed_time(dir_ev[k][j][a][1])
                                   for k in range(args.steps) for j in range(ITERS // EV_EVERY))
                   for a in range(3)]
     alg_bytes_step = BYTES_PER_POINT_AXIS * n ** 3 * 3 * ITERS
-    value = world * alg_bytes_step / (ms_step * 1e-3) / 1e9
+    value = whole_job_gbs(alg_bytes_step, ms_step, world)
 
     # ---- the same steps, each one CUDA graph of its 150 solves ----------------
     from adi import AdiGraph
@@ -233,10 +252,7 @@ def run_ours(args):
         g1.record(stream)
     torch.cuda.synchronize()
     graph_ms = g0.elapsed_time(g1) / args.steps
-    if world > 1:
-        t = torch.tensor([graph_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        graph_ms = float(t.item())
+    graph_ms = max_over_ranks(graph_ms, world, dev)
     adi_graph.close()
     del adi_graph
 
@@ -302,11 +318,8 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * alg_bytes_step / (e2e_ms * 1e-3) / 1e9
+    e2e_ms = max_over_ranks(e2e_ms, world, dev)
+    e2e_value = whole_job_gbs(alg_bytes_step, e2e_ms, world)
 
     # ---- roofline of the dominant kernel -------------------------------------
     dom = max(range(3), key=lambda a: per_dir_ms[a])
@@ -348,7 +361,7 @@ def run_ours(args):
                 "steps": e2e_steps,
                 "schedule": "pipelined: copies in of step k+1 and out of step k-1 overlap "
                             "the solves of step k (two device sets, two copy streams)"},
-        "graph": {"value": round(world * alg_bytes_step / (graph_ms * 1e-3) / 1e9, 2),
+        "graph": {"value": round(whole_job_gbs(alg_bytes_step, graph_ms, world), 2),
                   "unit": "GB/s", "ms_per_step": round(graph_ms, 4),
                   "note": "each step's 150 solves replayed as one CUDA graph (adi.AdiGraph)"},
         "gpu_launches": args.steps * ITERS * 3,
@@ -394,12 +407,9 @@ def run_ours(args):
         s1.record(stream)
     stream.synchronize()
     sf_ms = s0.elapsed_time(s1) / sf_steps
-    if world > 1:
-        t = torch.tensor([sf_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        sf_ms = float(t.item())
+    sf_ms = max_over_ranks(sf_ms, world, dev)
     sf_bytes = 2 * 8 * n ** 3 * 3 * ITERS
-    sf_gbs = world * sf_bytes / (sf_ms * 1e-3) / 1e9
+    sf_gbs = whole_job_gbs(sf_bytes, sf_ms, world)
     result["shared_fact"] = {
         "value": round(sf_gbs, 2), "unit": "GB/s", "ms_per_step": round(sf_ms, 4),
         "bytes_per_point_axis": 16, "frac_of_peak": round(sf_gbs / world / peak, 4),
