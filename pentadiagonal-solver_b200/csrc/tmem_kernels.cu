@@ -720,16 +720,25 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
           xb = xa;
           xa = xk[r];
         }
-        if (CONTIG && !JG.tma) {  // misaligned grid: each lane writes its own rows
-          if (active) {
-            F *const p = JG.x + (long long)(c0 + sys) * n;
-            const int row0 = part ? (mt + s * R) : (mt - 1 - s * R);
+        if (CONTIG && !JG.tma) {
+          // misaligned grid (no TMA): the step's results go through the
+          // shared tile and leave in runs of a line's R rows, R consecutive
+          // lanes a run, instead of one scattered element per lane
+          F *const ob = obuf;
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-              const int row = part ? row0 + r : row0 - r;
-              if (row < n) p[row] = xk[r];
-            }
+          for (int r = 0; r < R; ++r) ob[st1[r]] = xk[r];
+          __syncwarp();
+#pragma unroll 4
+          for (int k = 0; k < 2 * BOX / 32; ++k) {
+            const int idx = lane + 32 * k;
+            const int h = idx / BOX, rem = idx - h * BOX;
+            const int l = rem / R, rr = rem - l * R;
+            const int row = h ? (mt + s * R + rr) : (mt - (s + 1) * R + rr);
+            if (row < n && c0 + l < JG.n_sys)
+              JG.x[(long long)(c0 + l) * n + row] =
+                  ob[h * 2 * BOX + l * R + ((rr / EPC) ^ ((l >> 1) & 3)) * EPC + rr % EPC];
           }
+          __syncwarp();
         } else if (CONTIG) {
           F *const ob = obuf + o_buf * 4 * BOX;
           if ((s & 1) == 0 && s + 1 == n_stages) {  // a last step without a partner
