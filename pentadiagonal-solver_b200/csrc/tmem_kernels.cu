@@ -197,6 +197,11 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   __syncthreads();
   tmem_fence_after_sync();
   const uint32_t tmem_base = *tmem_slot;
+  // Programmatic dependent launch: the next grid in the stream may run its
+  // prologue on SMs this grid's CTAs leave; this grid touches global memory
+  // only after the previous grid has completed (everything above is on-chip)
+  if (threadIdx.x == 0) asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
 
   // the job of global tile t (t increases along a warp's sequence)
   auto job_of = [&](int t, int &cursor) -> const TmemJob<F> * {
@@ -923,7 +928,21 @@ cudaError_t tmem_launch_raw(const TmemJob<F> &job1, const TmemJob<F> *jobs, int 
   const int need = (total_tiles + NCONS - 1) / NCONS;
   const int grid = need < sm_count ? need : sm_count;
   if (grid <= 0) return cudaSuccess;
-  kern<<<grid, 96 * NCONS, G::kSmem, stream>>>(job1, jobs, n_jobs, total_tiles, flags, status);
+  // launched with programmatic stream serialization (see griddepcontrol in the
+  // kernel): at most one CTA per SM, all resident at once, so an early
+  // dependent only takes SMs this grid has left
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(96 * NCONS);
+  cfg.dynamicSmemBytes = G::kSmem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  err = cudaLaunchKernelEx(&cfg, kern, job1, jobs, n_jobs, total_tiles, flags, status);
+  if (err != cudaSuccess) return err;
   return cudaGetLastError();
 }
 
