@@ -170,3 +170,61 @@ def set_threads(n: int) -> None:
         gomp.omp_set_num_threads(ctypes.c_int(int(n)))
     except OSError:
         pass
+
+
+# --------------------------------------------------------------------------
+# The random test mesh (mesh_oracle.c) and the reference's own Mesh class
+# (_ref/libmesh_ref.so, ref_mesh_shim.cpp against include/util/mesh.hpp).
+# --------------------------------------------------------------------------
+REF_MESH_SO = HERE / "_ref" / "libmesh_ref.so"
+MESH_NAMES = ("ds", "dl", "d", "du", "dw", "x")
+
+
+def mt64_nth(seed: int, n: int) -> int:
+    """The n-th (1-based) output of MT19937-64 seeded with ``seed``."""
+    f = _oracle().penta_oracle_mt64_nth
+    f.argtypes = [ctypes.c_uint64, ctypes.c_longlong]
+    f.restype = ctypes.c_uint64
+    return int(f(seed, n))
+
+
+def _mesh_call(fn, dims, solvedim, nthreads, dtype) -> dict:
+    shape = tuple(reversed([int(v) for v in dims]))
+    out = {k: np.empty(shape, dtype=dtype) for k in MESH_NAMES}
+    fn.argtypes = [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [_P] * 6
+    fn.restype = ctypes.c_int
+    rc = fn(_dims_arr(dims), len(dims), int(solvedim), int(nthreads),
+            *(out[k].ctypes.data for k in MESH_NAMES))
+    if rc != 0:
+        raise ValueError(f"mesh generator rejected dims={dims} solvedim={solvedim}")
+    return out
+
+
+def mesh_random(dims, solvedim: int, nthreads: int, dtype=np.float64) -> dict:
+    """The reference's random grid for ``nthreads`` OpenMP threads (restatement)."""
+    suf = "d" if np.dtype(dtype) == np.float64 else "s"
+    return _mesh_call(getattr(_oracle(), f"penta_oracle_mesh_random_{suf}"), dims, solvedim,
+                      nthreads, dtype)
+
+
+def ref_mesh_available() -> bool:
+    return REF_MESH_SO.exists()
+
+
+def ref_mesh_random(dims, solvedim: int, nthreads: int, dtype=np.float64) -> dict:
+    """``Mesh<Float>(solvedim, dims)`` itself, run with ``nthreads`` threads."""
+    suf = "d" if np.dtype(dtype) == np.float64 else "s"
+    return _mesh_call(getattr(_load(REF_MESH_SO), f"ref_mesh_random_{suf}"), dims, solvedim,
+                      nthreads, dtype)
+
+
+def ref_mesh_load(path, dims, dtype=np.float64) -> dict:
+    """``Mesh<Float>(file)`` itself: ds .. x and u of a fixture file."""
+    suf = "d" if np.dtype(dtype) == np.float64 else "s"
+    fn = getattr(_load(REF_MESH_SO), f"ref_mesh_load_{suf}")
+    fn.argtypes = [ctypes.c_char_p] + [_P] * 7
+    fn.restype = ctypes.c_int
+    shape = tuple(reversed([int(v) for v in dims]))
+    out = {k: np.empty(shape, dtype=dtype) for k in MESH_NAMES + ("u",)}
+    fn(os.fsencode(str(path)), *(out[k].ctypes.data for k in MESH_NAMES + ("u",)))
+    return out

@@ -18,10 +18,19 @@
            latency and solves/s for the mixed and FP64 policies and for
            sequential plain FP64 calls, at that rate and at saturation.
 
-All inputs are synthetic (seeded); times are CUDA-event device times except
-the serving loop (wall clock, as a client sees it).
+  mesh     the reference's random benchmark grid, 256^3 FP64 (the largest of
+           benchmarks/cuda/my_bm.cu), built on the device by
+           pentadsolver_D_mesh_random for several host thread counts, against
+           the reference's own path: Mesh<double>(2, dims) on the host cores
+           (include/util/mesh.hpp:85-124, compiled from the reference tree
+           into oracle/_ref) with the same thread count, then the upload of
+           its six arrays from pageable memory (device_mesh.hpp:52-65).  The
+           device grid is compared with the reference's bit for bit.
 
-  python pentadiagonal-solver_b200/bench_configs.py [--configs 0,2,3,4]
+All inputs are synthetic (seeded); times are CUDA-event device times except
+the serving loop and the reference's host mesh build (wall clock).
+
+  python pentadiagonal-solver_b200/bench_configs.py [--configs 0,2,3,4,mesh]
 """
 from __future__ import annotations
 
@@ -324,6 +333,51 @@ def config4(rate=2000.0, seconds=2.0, n_problems=64, budget=150e9, seed=44):
     return out
 
 
+def config_mesh(edge=256):
+    import torch
+
+    import mesh
+    from oracle import oracle
+
+    dims = (edge, edge, edge)
+    solvedim = 2
+    n_bytes = 6 * edge ** 3 * 8
+    res = {"config": f"mesh_random_{edge}cube_fp64", "bytes": n_bytes,
+           "host_threads": mesh.host_threads()}
+    dev = {}
+    for threads in sorted({mesh.host_threads(), 64, 148, 1024}):
+        holder = {}
+
+        def build():
+            holder["m"] = mesh.random_mesh(dims, solvedim, threads, torch.float64)
+        ms = timed(build, reps=3, warmup=1)
+        dev[threads] = {"ms": round(ms, 3), "gbs": round(n_bytes / ms / 1e6, 1)}
+        holder.clear()
+    res["device_build"] = {str(k): v for k, v in dev.items()}
+    if oracle.ref_mesh_available():
+        t = mesh.host_threads()
+        oracle.set_threads(t)
+        t0 = time.time()
+        ref = oracle.ref_mesh_random(dims, solvedim, t, np.float64)
+        res["reference_host_build_ms"] = round((time.time() - t0) * 1e3, 1)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        up = {k: torch.from_numpy(ref[k]).to("cuda") for k in NAMES}
+        torch.cuda.synchronize()
+        res["reference_upload_ms"] = round((time.time() - t0) * 1e3, 1)
+        got = mesh.random_mesh(dims, solvedim, t, torch.float64)
+        torch.cuda.synchronize()
+        res["bit_identical_to_reference"] = all(torch.equal(got[k].view(torch.int64),
+                                                            up[k].view(torch.int64))
+                                                for k in NAMES)
+        res["reference_total_ms"] = round(res["reference_host_build_ms"] +
+                                          res["reference_upload_ms"], 1)
+        res["speedup_same_threads"] = round(res["reference_total_ms"] / dev[t]["ms"], 1)
+    else:
+        res["reference"] = "oracle/_ref/libmesh_ref.so not built"
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--configs", default="0,2,3,4")
@@ -333,8 +387,8 @@ def main():
     args = ap.parse_args()
     want = {c.strip() for c in args.configs.split(",")}
     runs = {"0": config0, "2": lambda: config2(args.n2), "3": lambda: config3(args.grids3),
-            "4": lambda: config4(seconds=args.seconds4)}
-    for c in ("0", "2", "3", "4"):
+            "4": lambda: config4(seconds=args.seconds4), "mesh": config_mesh}
+    for c in ("0", "2", "3", "4", "mesh"):
         if c in want:
             t0 = time.time()
             res = runs[c]()
