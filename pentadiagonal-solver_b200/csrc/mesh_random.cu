@@ -23,10 +23,12 @@
 // for mt19937_64) keeps 312 words; a refill computes word k from words k,
 // k+1 and k+156, so 156 lanes produce all 312 new words in one step: lane k
 // makes word k from old words and word k+156 from its own new word k (and, for
-// the last word, from a second copy of new word 0).  Each lane then tempers
-// its two words, turns them into the two draws they are (draw index ->
-// system, row, array) and stores them.  A stream is sequential, so a CTA
-// emits 312 draws per step; the grid's time is set by draws per host thread.
+// the last word, from a second copy of new word 0).  A batch refills 8 steps
+// into a ring in shared memory (one barrier per step, little work), then 624
+// threads temper and place its 2496 draws with no barrier between them: each
+// keeps a cursor (system, draw within the system, first element) that moves
+// 624 draws at a time without a division, and finds the row in closed form.
+// A stream is sequential, so the grid's time is set by draws per host thread.
 // The canonical conversion is libstdc++'s generate_canonical with one 64-bit
 // draw: u = (Float)v * 2^-64 rounded to nearest (an exact scaling), and the
 // largest Float below 1 when the conversion rounds up to 2^64.
@@ -42,7 +44,11 @@ namespace {
 
 constexpr int kMtN = 312;
 constexpr int kMtHalf = 156;
-constexpr int kMeshThreads = 160;  // 156 working lanes, five warps
+constexpr int kSteps = 8;           // generator steps refilled per batch
+constexpr int kPerWord = 2;         // placing threads per word position
+constexpr int kPlacers = kPerWord * kMtN;
+constexpr int kMeshThreads = 640;   // 624 placing threads, 156 of them also refill
+static_assert(kSteps % kPerWord == 0, "each placing thread takes every kPerWord-th step");
 
 struct MeshShape {
   long long inner;   // product of dims below solvedim (row stride)
@@ -94,20 +100,79 @@ template <typename F> struct MeshOut {
   }
 };
 
-// Stores draw number g (0-based) of host thread t's stream: value v.
-template <typename F>
-__device__ __forceinline__ void place(const MeshShape &s, long long lo, long long g, F v,
-                                      const MeshOut<F> &out) {
-  const long long sys = lo + g / s.per_sys;
-  const long long e = g % s.per_sys;
-  // row: the largest r with draws_before(r) <= e (each row draws at least twice)
-  long long a = 0, b = s.n;
+// Where draw e of a system falls: its row r and k, the draw's rank in the row.
+// For n >= 4 the rows have 4, 5, 6, ..., 6, 5, 4 draws (row r >= 2 starts at
+// draw 6r - 3 up to row n-2); shorter systems search the prefix counts.
+__device__ __forceinline__ void row_of(long long e, long long n, long long &r, int &k) {
+  if (n >= 4) {
+    if (e < 4) {
+      r = 0;
+      k = static_cast<int>(e);
+    } else if (e < 9) {
+      r = 1;
+      k = static_cast<int>(e - 4);
+    } else if (e < 6 * n - 15) {
+      const unsigned long long q = static_cast<unsigned long long>(e + 3) / 6ull;
+      r = static_cast<long long>(q);
+      k = static_cast<int>(e + 3 - 6 * r);
+    } else if (e < 6 * n - 10) {
+      r = n - 2;
+      k = static_cast<int>(e - (6 * n - 15));
+    } else {
+      r = n - 1;
+      k = static_cast<int>(e - (6 * n - 10));
+    }
+    return;
+  }
+  long long a = 0, b = n;  // the largest a with draws_before(a) <= e
   while (b - a > 1) {
     const long long mid = (a + b) >> 1;
-    if (draws_before(mid, s.n) <= e) a = mid; else b = mid;
+    if (draws_before(mid, n) <= e) a = mid; else b = mid;
   }
-  const long long r = a;
-  const int k = static_cast<int>(e - draws_before(r, s.n));
+  r = a;
+  k = static_cast<int>(e - draws_before(a, n));
+}
+
+// A lane's position in its host thread's stream: draw e of system `sys`, whose
+// first element is `start` (= i * inner * n + j for sys = i * inner + j).
+struct Cursor {
+  long long sys, e, j, start;
+};
+
+__device__ __forceinline__ void cursor_set(Cursor &c, const MeshShape &s, long long sys,
+                                           long long e) {
+  const long long i = sys / s.inner;
+  c.sys = sys;
+  c.e = e;
+  c.j = sys - i * s.inner;
+  c.start = i * s.inner * s.n + c.j;
+}
+
+// Moves the cursor `step` draws on; one system ahead at most without a division.
+__device__ __forceinline__ void cursor_advance(Cursor &c, const MeshShape &s, long long step) {
+  c.e += step;
+  if (c.e < s.per_sys) return;
+  if (c.e - s.per_sys < s.per_sys) {
+    c.e -= s.per_sys;
+    ++c.sys;
+    ++c.start;
+    if (++c.j == s.inner) {
+      c.j = 0;
+      c.start += s.inner * (s.n - 1);
+    }
+    return;
+  }
+  const long long w = c.e / s.per_sys;
+  cursor_set(c, s, c.sys + w, c.e - w * s.per_sys);
+}
+
+// Stores the draw under cursor c, value v.
+template <typename F>
+__device__ __forceinline__ void place(const MeshShape &s, const Cursor &c, F v,
+                                      const MeshOut<F> &out) {
+  long long r;
+  int k;
+  row_of(c.e, s.n, r, k);
   const bool has[6] = {r > 1, r > 0, true, r < s.n - 1,
                        s.n >= 2 ? r < s.n - 2 : true, true};
   int slot = 0;
@@ -115,8 +180,7 @@ __device__ __forceinline__ void place(const MeshShape &s, long long lo, long lon
     seen += has[slot] ? 1 : 0;
     if (seen == k) break;
   }
-  const long long i = sys / s.inner, j = sys - i * s.inner;
-  const long long idx = i * s.inner * s.n + j + r * s.inner;
+  const long long idx = c.start + r * s.inner;
   out.pick(slot)[idx] = slot == 2 ? F(6) * v : (slot == 5 ? v : -v);
   if (slot == 2) {
     // the row's entries that take no draw, written once per row
@@ -129,7 +193,9 @@ __device__ __forceinline__ void place(const MeshShape &s, long long lo, long lon
 template <typename F>
 __global__ void __launch_bounds__(kMeshThreads)
 mesh_random_kernel(MeshShape s, F *ds, F *dl, F *d, F *du, F *dw, F *x) {
-  __shared__ uint64_t mt[kMtN];
+  // the untempered words of the batch's steps; before the first batch the last
+  // slot holds the seeded state
+  __shared__ uint64_t ring[kSteps][kMtN];
   const MeshOut<F> out{{ds, dl, d, du, dw, x}};
   const long long t = blockIdx.x;
   const long long q = s.count / s.threads, rem = s.count % s.threads;
@@ -140,33 +206,48 @@ mesh_random_kernel(MeshShape s, F *ds, F *dl, F *d, F *du, F *dw, F *x) {
 
   if (k == 0) {
     uint64_t w = static_cast<uint64_t>(t);
-    mt[0] = w;
+    ring[kSteps - 1][0] = w;
     for (int i = 1; i < kMtN; ++i) {
       w = 6364136223846793005ull * (w ^ (w >> 62)) + static_cast<uint64_t>(i);
-      mt[i] = w;
+      ring[kSteps - 1][i] = w;
     }
+  }
+  // Thread k < 624 places word `word` of steps half, half + 2, ... of every
+  // batch: draws half * 312 + word + 624 j of the stream.
+  const int word = k % kMtN, half = k / kMtN;
+  Cursor c;
+  {
+    const long long g = static_cast<long long>(half) * kMtN + word;
+    cursor_set(c, s, lo + g / s.per_sys, g % s.per_sys);
   }
   __syncthreads();
 
-  for (long long base = 0; base < total; base += kMtN) {
-    uint64_t lo_new = 0, hi_new = 0;
-    if (k < kMtHalf) {
-      const uint64_t a0 = mt[k], a1 = mt[k + 1], b0 = mt[k + kMtHalf];
-      // word k + 157 is old, except after the last word, where it is new word 0
-      const uint64_t b1 = k + 1 < kMtHalf ? mt[k + kMtHalf + 1]
-                                          : mt_mix(mt[0], mt[1], mt[kMtHalf]);
-      lo_new = mt_mix(a0, a1, b0);
-      hi_new = mt_mix(b0, b1, lo_new);
+  for (long long base = 0; base < total; base += kSteps * kMtN) {
+    // Refill: step st from step st - 1 (the previous batch's last for st = 0).
+    // Lane k makes word k and word k + 156; word k + 157 is old, except after
+    // the last word, where it is new word 0 (made again here from old words).
+#pragma unroll 1
+    for (int st = 0; st < kSteps; ++st) {
+      const uint64_t *prev = ring[(st + kSteps - 1) % kSteps];
+      if (k < kMtHalf) {
+        const uint64_t a0 = prev[k], a1 = prev[k + 1], b0 = prev[k + kMtHalf];
+        const uint64_t b1 = k + 1 < kMtHalf ? prev[k + kMtHalf + 1]
+                                            : mt_mix(prev[0], prev[1], prev[kMtHalf]);
+        const uint64_t lo_new = mt_mix(a0, a1, b0);
+        ring[st][k] = lo_new;
+        ring[st][k + kMtHalf] = mt_mix(b0, b1, lo_new);
+      }
+      __syncthreads();
     }
-    __syncthreads();  // every old word read before any is replaced
-    if (k < kMtHalf) {
-      mt[k] = lo_new;
-      mt[k + kMtHalf] = hi_new;
-      const long long g0 = base + k, g1 = base + kMtHalf + k;
-      if (g0 < total) place<F>(s, lo, g0, canonical<F>(mt_temper(lo_new)), out);
-      if (g1 < total) place<F>(s, lo, g1, canonical<F>(mt_temper(hi_new)), out);
+    if (k < kPlacers) {
+#pragma unroll
+      for (int st = 0; st < kSteps; st += kPerWord) {
+        const long long g = base + static_cast<long long>(st + half) * kMtN + word;
+        if (g < total) place<F>(s, c, canonical<F>(mt_temper(ring[st + half][word])), out);
+        cursor_advance(c, s, kPlacers);
+      }
     }
-    __syncthreads();  // the new words are in place before the next refill
+    __syncthreads();  // the batch is placed before its slots are refilled
   }
 }
 
