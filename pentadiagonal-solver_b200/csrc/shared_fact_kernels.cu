@@ -202,7 +202,14 @@ sf_tmem_kernel(const __grid_constant__ CUtensorMap xmap, const F *__restrict__ d
         }
       }
   };
+  // Programmatic dependent launch: the next solve on the stream may start its
+  // on-chip prologue on SMs this grid has left; every global access of this
+  // grid comes after griddepcontrol.wait (the previous grid complete and its
+  // writes visible) -- the builder's before its first read, the others' after
+  // the prologue.
+  if (threadIdx.x == 0) asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   if (builder) {
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
     if (cache != nullptr && lane == 0) {
       const unsigned comp = (unsigned)(mt * sizeof(F));
       mbar_init(cbar, 1);
@@ -235,6 +242,7 @@ sf_tmem_kernel(const __grid_constant__ CUtensorMap xmap, const F *__restrict__ d
   __syncthreads();
   tmem_fence_after_sync();
   const uint32_t tmem_base = *tmem_slot;
+  if (!builder) asm volatile("griddepcontrol.wait;\n" ::: "memory");
 
   // ================================ builder =================================
   if (builder) {
@@ -759,9 +767,20 @@ cudaError_t sf_tmem_launch(const SolveArgs<F> &a, int sm_count, size_t usable_bu
   }
   const long long need = (n_tiles + NCONS - 1) / NCONS;
   const int grid = (int)(need < sm_count ? need : sm_count);
-  kern<<<grid, 32 * (2 * NCONS + 1), G::kSmem, stream>>>(xmap, a.ds, a.dl, a.d, a.du, a.dw, a.x,
-                                                     cache, n, mt, inner, tpr,
-                                                     (int)a.L.n_sys, (int)n_tiles, a.status);
+  // programmatic stream serialization: see the kernel's griddepcontrol.wait
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(32 * (2 * NCONS + 1));
+  cfg.dynamicSmemBytes = G::kSmem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  err = cudaLaunchKernelEx(&cfg, kern, xmap, a.ds, a.dl, a.d, a.du, a.dw, a.x, cache, n, mt,
+                           inner, tpr, (int)a.L.n_sys, (int)n_tiles, a.status);
+  if (err != cudaSuccess) return err;
   return cudaGetLastError();
 }
 
