@@ -28,9 +28,12 @@
            device grid is compared with the reference's bit for bit.
 
 All inputs are synthetic (seeded); times are CUDA-event device times except
-the serving loop and the reference's host mesh build (wall clock).
+the serving loop and the reference's host mesh build (wall clock).  Like
+bench.py, this script uses oracle/ only as the checker (forward errors) and
+for the reference's own CPU code timed as the baseline; the solves and grids
+it measures are the library's.
 
-  python pentadiagonal-solver_b200/bench_configs.py [--configs 0,2,3,4,mesh]
+  python bench_configs.py [--configs 0,2,3,4,mesh]
 """
 from __future__ import annotations
 
@@ -41,8 +44,8 @@ import sys
 import time
 from pathlib import Path
 
-HERE = Path(__file__).resolve().parent
-REPO = HERE.parent
+REPO = Path(__file__).resolve().parent
+HERE = REPO / "pentadiagonal-solver_b200"
 for p in (str(HERE), str(REPO), str(REPO / "tests")):
     if p not in sys.path:
         sys.path.insert(0, p)
