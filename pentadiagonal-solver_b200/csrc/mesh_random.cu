@@ -18,17 +18,23 @@
 // it as `n_threads` and write, straight into device arrays, the grid the
 // reference builds with that many threads -- bit for bit, in FP64 and FP32.
 //
-// Device design: one CTA per host thread replays that thread's generator.
-// MT19937-64 (Matsumoto and Nishimura; the parameters the C++ standard fixes
-// for mt19937_64) keeps 312 words; a refill computes word k from words k,
-// k+1 and k+156, so 156 lanes produce all 312 new words in one step: lane k
-// makes word k from old words and word k+156 from its own new word k (and, for
-// the last word, from a second copy of new word 0).  A batch refills 8 steps
-// into a ring in shared memory (one barrier per step, little work), then 624
-// threads temper and place its 2496 draws with no barrier between them: each
-// keeps a cursor (system, draw within the system, first element) that moves
-// 624 draws at a time without a division, and finds the row in closed form.
-// A stream is sequential, so the grid's time is set by draws per host thread.
+// Device design: a cluster of up to 8 CTAs per host thread replays that
+// thread's generator.  MT19937-64 (Matsumoto and Nishimura; the parameters the
+// C++ standard fixes for mt19937_64) keeps 312 words; a refill computes word k
+// from words k, k+1 and k+156, so 156 lanes produce all 312 new words in one
+// step: lane k makes word k from old words and word k+156 from its own new
+// word k (and, for the last word, from a second copy of new word 0).  Five
+// warps of the cluster's first CTA refill 32 steps (9,984 draws) at a time
+// into a double-buffered ring in its shared memory, one batch ahead, with a
+// named barrier between steps; meanwhile 624 threads of every CTA of the
+// cluster temper and place the current batch, reading the ring through
+// distributed shared memory.  Each placing thread keeps a cursor (system, draw
+// within the system, first element) that moves a fixed number of draws at a
+// time without a division, and finds the row in closed form.  One cluster
+// barrier per batch.  A stream is sequential: the time is set by the refill
+// chain of one host thread.  The cluster width is the widest of which the
+// device holds one per host thread at once (cudaOccupancyMaxActiveClusters):
+// a second wave of clusters would double the time.
 // The canonical conversion is libstdc++'s generate_canonical with one 64-bit
 // draw: u = (Float)v * 2^-64 rounded to nearest (an exact scaling), and the
 // largest Float below 1 when the conversion rounds up to 2^64.
@@ -36,6 +42,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 
 #include "pentad_common.hpp"
 #include "pentadsolver_mesh.h"
@@ -44,11 +51,15 @@ namespace {
 
 constexpr int kMtN = 312;
 constexpr int kMtHalf = 156;
-constexpr int kSteps = 8;           // generator steps refilled per batch
-constexpr int kPerWord = 2;         // placing threads per word position
-constexpr int kPlacers = kPerWord * kMtN;
-constexpr int kMeshThreads = 640;   // 624 placing threads, 156 of them also refill
-static_assert(kSteps % kPerWord == 0, "each placing thread takes every kPerWord-th step");
+constexpr int kSteps = 32;                  // generator steps per batch
+constexpr int kBatch = kSteps * kMtN;       // draws per batch (9984)
+constexpr int kPlacers = 624;               // placing threads per CTA
+constexpr int kPlaceWarps = 20;             // warps 0-19 place (624 of their 640 lanes)
+constexpr int kRefillWarps = 5;             // warps 20-24 refill (156 of 160 lanes)
+constexpr int kMeshThreads = 32 * (kPlaceWarps + kRefillWarps);
+constexpr int kMaxCluster = 8;
+constexpr size_t kRingBytes = 2ull * kBatch * sizeof(uint64_t);  // two batches
+static_assert(kBatch % (kPlacers * kMaxCluster) == 0, "placers of a cluster tile a batch");
 
 struct MeshShape {
   long long inner;   // product of dims below solvedim (row stride)
@@ -190,65 +201,162 @@ __device__ __forceinline__ void place(const MeshShape &s, const Cursor &c, F v,
   }
 }
 
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned cluster_size() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+// Every thread of every CTA of the cluster.  `release`: this thread's writes
+// before it (the ring's shared memory) are visible to the cluster's reads after
+// it.  Without it the arrive orders nothing -- the placing threads' loads are
+// consumed before it anyway, and their scattered global stores need not drain
+// at every batch.
+__device__ __forceinline__ void cluster_sync_all(bool release) {
+  __syncwarp();  // the .aligned forms want the whole warp converged
+  if (release)
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+  else
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ uint64_t ld_cluster_u64(uint32_t addr) {
+  uint64_t v;
+  asm volatile("ld.shared::cluster.u64 %0, [%1];" : "=l"(v) : "r"(addr) : "memory");
+  return v;
+}
+__device__ __forceinline__ void refill_sync() {  // the five refilling warps only
+  asm volatile("bar.sync 1, %0;" ::"n"(32 * kRefillWarps) : "memory");
+}
+
+// Steps 0 .. kSteps-1 of one batch into `cur`; step 0 follows `prev_last`.
+// Lane k makes word k from old words and word k + 156 from its own new word k;
+// word k + 157 is old except after the last word, where it is new word 0 (made
+// again here from old words).
+__device__ __forceinline__ void refill(uint64_t *cur, const uint64_t *prev_last, int k) {
+#pragma unroll 1
+  for (int st = 0; st < kSteps; ++st) {
+    const uint64_t *prev = st == 0 ? prev_last : cur + (st - 1) * kMtN;
+    uint64_t *out = cur + st * kMtN;
+    if (k < kMtHalf) {
+      const uint64_t a0 = prev[k], a1 = prev[k + 1], b0 = prev[k + kMtHalf];
+      const uint64_t b1 = k + 1 < kMtHalf ? prev[k + kMtHalf + 1]
+                                          : mt_mix(prev[0], prev[1], prev[kMtHalf]);
+      const uint64_t lo_new = mt_mix(a0, a1, b0);
+      out[k] = lo_new;
+      out[k + kMtHalf] = mt_mix(b0, b1, lo_new);
+    }
+    refill_sync();
+  }
+}
+
+// One host thread's stream per cluster of C CTAs (C = 1, 2, 4 or 8; blocks
+// [t C, t C + C) replay thread t).  Warps 20-24 of the cluster's first CTA
+// refill a double-buffered ring of batches in its shared memory, one batch
+// ahead; warps 0-19 of every CTA place the current batch, reading the ring
+// over distributed shared memory: placing thread p = rank * 624 + lane takes
+// batch draws p, p + 624 C, ... (16 / C of them), so its draws in the stream
+// are 624 C apart.  One cluster barrier per batch.
 template <typename F>
-__global__ void __launch_bounds__(kMeshThreads)
+__global__ void __launch_bounds__(kMeshThreads, 1)
 mesh_random_kernel(MeshShape s, F *ds, F *dl, F *d, F *du, F *dw, F *x) {
-  // the untempered words of the batch's steps; before the first batch the last
-  // slot holds the seeded state
-  __shared__ uint64_t ring[kSteps][kMtN];
+  extern __shared__ __align__(16) uint64_t ring[];  // [2][kSteps][312], first CTA only
   const MeshOut<F> out{{ds, dl, d, du, dw, x}};
-  const long long t = blockIdx.x;
+  const unsigned rank = cluster_rank(), csize = cluster_size();
+  const long long t = blockIdx.x / csize;
   const long long q = s.count / s.threads, rem = s.count % s.threads;
   const long long lo = q * t + (t < rem ? t : rem);
   const long long total = (q + (t < rem ? 1 : 0)) * s.per_sys;
-  if (total == 0) return;
-  const int k = threadIdx.x;
+  if (total == 0) return;  // the whole cluster (same t) leaves
+  const int warp = threadIdx.x / 32;
+  const bool refiller = rank == 0 && warp >= kPlaceWarps;
+  const int rk = threadIdx.x - 32 * kPlaceWarps;  // lane within the refilling warps
+  const int p_local = threadIdx.x;                // placing thread within the CTA
+  const long long stride = (long long)kPlacers * csize;
+  const int per_batch = kBatch / (int)stride;     // draws per placing thread per batch
+  const long long p = (long long)rank * kPlacers + p_local;
 
-  if (k == 0) {
-    uint64_t w = static_cast<uint64_t>(t);
-    ring[kSteps - 1][0] = w;
-    for (int i = 1; i < kMtN; ++i) {
-      w = 6364136223846793005ull * (w ^ (w >> 62)) + static_cast<uint64_t>(i);
-      ring[kSteps - 1][i] = w;
+  if (refiller) {
+    // seed into the last step of buffer 1, then batch 0 into buffer 0
+    uint64_t *seed = ring + kBatch + (kSteps - 1) * kMtN;
+    if (rk == 0) {
+      uint64_t w = static_cast<uint64_t>(t);
+      seed[0] = w;
+      for (int i = 1; i < kMtN; ++i) {
+        w = 6364136223846793005ull * (w ^ (w >> 62)) + static_cast<uint64_t>(i);
+        seed[i] = w;
+      }
     }
+    refill_sync();
+    refill(ring, seed, rk);
   }
-  // Thread k < 624 places word `word` of steps half, half + 2, ... of every
-  // batch: draws half * 312 + word + 624 j of the stream.
-  const int word = k % kMtN, half = k / kMtN;
   Cursor c;
-  {
-    const long long g = static_cast<long long>(half) * kMtN + word;
-    cursor_set(c, s, lo + g / s.per_sys, g % s.per_sys);
-  }
-  __syncthreads();
+  if (p_local < kPlacers) cursor_set(c, s, lo + p / s.per_sys, p % s.per_sys);
+  uint32_t ring0;  // the ring in the first CTA's shared memory
+  asm volatile("mapa.shared::cluster.u32 %0, %1, 0;"
+               : "=r"(ring0) : "r"((uint32_t)__cvta_generic_to_shared(ring)));
+  cluster_sync_all(refiller);
 
-  for (long long base = 0; base < total; base += kSteps * kMtN) {
-    // Refill: step st from step st - 1 (the previous batch's last for st = 0).
-    // Lane k makes word k and word k + 156; word k + 157 is old, except after
-    // the last word, where it is new word 0 (made again here from old words).
-#pragma unroll 1
-    for (int st = 0; st < kSteps; ++st) {
-      const uint64_t *prev = ring[(st + kSteps - 1) % kSteps];
-      if (k < kMtHalf) {
-        const uint64_t a0 = prev[k], a1 = prev[k + 1], b0 = prev[k + kMtHalf];
-        const uint64_t b1 = k + 1 < kMtHalf ? prev[k + kMtHalf + 1]
-                                            : mt_mix(prev[0], prev[1], prev[kMtHalf]);
-        const uint64_t lo_new = mt_mix(a0, a1, b0);
-        ring[st][k] = lo_new;
-        ring[st][k + kMtHalf] = mt_mix(b0, b1, lo_new);
-      }
-      __syncthreads();
-    }
-    if (k < kPlacers) {
-#pragma unroll
-      for (int st = 0; st < kSteps; st += kPerWord) {
-        const long long g = base + static_cast<long long>(st + half) * kMtN + word;
-        if (g < total) place<F>(s, c, canonical<F>(mt_temper(ring[st + half][word])), out);
-        cursor_advance(c, s, kPlacers);
+  long long b = 0;
+  for (long long base = 0; base < total; base += kBatch, ++b) {
+    const int buf = (int)(b & 1);
+    if (refiller && base + kBatch < total)
+      refill(ring + (buf ^ 1) * kBatch, ring + buf * kBatch + (kSteps - 1) * kMtN, rk);
+    if (p_local < kPlacers) {
+      for (int i = 0; i < per_batch; ++i) {
+        const long long j = p + stride * i;  // draw within the batch
+        const long long g = base + j;
+        if (g < total) {
+          const uint64_t w = ld_cluster_u64(ring0 + (uint32_t)((buf * kBatch + j) * 8));
+          place<F>(s, c, canonical<F>(mt_temper(w)), out);
+        }
+        cursor_advance(c, s, stride);
       }
     }
-    __syncthreads();  // the batch is placed before its slots are refilled
+    cluster_sync_all(refiller);  // batch placed and the next one refilled
   }
+}
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+// [FP32, FP64][device][cluster width 1, 2, 4, 8]: clusters the device can hold
+// at once (0 = not yet known, -1 = cannot launch)
+int g_active[2][kMaxDevices][4] = {};
+
+// How many clusters of `width` CTAs the device runs at once, found once per
+// device, precision and width (clusters of 8 CTAs need 8 free SMs of one GPC,
+// so fewer fit than SMs / 8).
+template <typename F> int active_clusters(int dev, int width) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  int &a = g_active[sizeof(F) == 8][dev][width == 8 ? 3 : width / 2];
+  if (a != 0) return a;
+  a = -1;
+  auto kern = mesh_random_kernel<F>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kRingBytes) != cudaSuccess) {
+    cudaGetLastError();
+    return a;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)width);
+  cfg.blockDim = dim3(kMeshThreads);
+  cfg.dynamicSmemBytes = kRingBytes;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)width;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) == cudaSuccess && clusters > 0)
+    a = clusters;
+  cudaGetLastError();
+  return a;
 }
 
 template <typename F>
@@ -272,9 +380,38 @@ pentadStatus_t mesh_random(const int *dims, int ndims, int solvedim, int n_threa
     const long long dwn = n >= 2 ? (r < n - 2 ? r : n - 2) : r;
     s.per_sys = 2 * r + dsn + dln + dun + dwn;
   }
-  mesh_random_kernel<F><<<n_threads, kMeshThreads, 0, static_cast<cudaStream_t>(stream)>>>(
-      s, ds, dl, d, du, dw, x);
-  if (cudaGetLastError() != cudaSuccess) return PENTAD_STATUS_EXECUTION_FAILED;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return PENTAD_STATUS_NOT_INITIALIZED;
+  }
+  auto kern = mesh_random_kernel<F>;
+  // CTAs per host thread: the widest cluster (8, 4, 2) of which the device
+  // holds one per host thread at once; else one CTA per host thread
+  int csize = 1;
+  for (int w = kMaxCluster; w > 1; w /= 2)
+    if (active_clusters<F>(dev, w) >= n_threads) {
+      csize = w;
+      break;
+    }
+  if (csize == 1 && active_clusters<F>(dev, 1) < 1) return PENTAD_STATUS_EXECUTION_FAILED;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(n_threads * csize));
+  cfg.blockDim = dim3(kMeshThreads);
+  cfg.dynamicSmemBytes = kRingBytes;
+  cfg.stream = static_cast<cudaStream_t>(stream);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)csize;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (cudaLaunchKernelEx(&cfg, kern, s, ds, dl, d, du, dw, x) != cudaSuccess ||
+      cudaGetLastError() != cudaSuccess) {
+    cudaGetLastError();
+    return PENTAD_STATUS_EXECUTION_FAILED;
+  }
   return PENTAD_STATUS_SUCCESS;
 }
 
