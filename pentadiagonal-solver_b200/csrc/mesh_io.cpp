@@ -162,6 +162,7 @@ bool parse_array(const char *&p, const char *end, long long n, F *out) {
 template <typename F>
 pentadStatus_t fixture_read(const char *path, F *ds, F *dl, F *d, F *du, F *dw, F *x, F *u) {
   if (!path || !ds || !dl || !d || !du || !dw || !x) return PENTAD_STATUS_INVALID_VALUE;
+  if (c_locale() == static_cast<locale_t>(0)) return PENTAD_STATUS_INTERNAL_ERROR;
   std::string buf;
   if (!read_file(path, buf)) {
     complain(path, "cannot be read");
@@ -229,6 +230,7 @@ pentadStatus_t fixture_write(const char *path, int format, int ndims, int solved
   if (!path || !dims || !ds || !dl || !d || !du || !dw || !x) return PENTAD_STATUS_INVALID_VALUE;
   if (format != PENTADSOLVER_FIXTURE_TEXT && format != static_cast<int>(sizeof(F)))
     return PENTAD_STATUS_INVALID_VALUE;
+  if (c_locale() == static_cast<locale_t>(0)) return PENTAD_STATUS_INTERNAL_ERROR;
   Header h;
   h.ndims = ndims;
   h.solvedim = solvedim;
@@ -290,6 +292,7 @@ extern "C" PENTAD_API pentadStatus_t pentadsolver_fixture_info(const char *path,
                                                                int *solvedim, int *dims,
                                                                int *format) {
   if (!path || !ndims || !solvedim || !dims || !format) return PENTAD_STATUS_INVALID_VALUE;
+  if (c_locale() == static_cast<locale_t>(0)) return PENTAD_STATUS_INTERNAL_ERROR;
   std::string buf;
   if (!read_file(path, buf)) {
     complain(path, "cannot be read");
