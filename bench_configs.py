@@ -27,13 +27,22 @@
            its six arrays from pageable memory (device_mesh.hpp:52-65).  The
            device grid is compared with the reference's bit for bit.
 
+  refapp   the reference's own ADI benchmark, apps/adi_cuda.cu unchanged, 256^3,
+           50 timed iterations after its 1.5 s warm-up, built twice by
+           oracle/Makefile: on the reference's GPU solver (app_cuda_ref) and on
+           this library (app_cuda_b200); FP64 and FP32 with the default
+           selectors, and FP64 with shared factorisation.  Its constant
+           coefficients (1, 1, 5, 1, 1; RHS 1) are the app's own.  GB/s =
+           algorithmic bytes of the three solves per iteration over the app's
+           CUDA-event iteration time.
+
 All inputs are synthetic (seeded); times are CUDA-event device times except
 the serving loop and the reference's host mesh build (wall clock).  Like
 bench.py, this script uses oracle/ only as the checker (forward errors) and
 for the reference's own CPU code timed as the baseline; the solves and grids
 it measures are the library's.
 
-  python bench_configs.py [--configs 0,2,3,4,mesh]
+  python bench_configs.py [--configs 0,2,3,4,mesh,refapp]
 """
 from __future__ import annotations
 
@@ -381,6 +390,46 @@ def config_mesh(edge=256):
     return res
 
 
+def config_refapp(edge=256, iters=50):
+    import os
+    import subprocess
+
+    ref_dir = REPO / "oracle" / "_ref"
+    apps = {"reference": ref_dir / "app_cuda_ref", "b200": ref_dir / "app_cuda_b200"}
+    missing = [str(v) for v in apps.values() if not v.exists()]
+    if missing:
+        return {"config": "refapp", "unavailable": f"not built: {missing}"}
+    runs = [("double", {}), ("float", {}),
+            ("double", {"PENTA_XALGO": "shared-fact", "PENTA_YZALGO": "shared-fact"})]
+    out = {"config": f"reference_adi_app_{edge}cube", "iters": iters, "runs": []}
+    for prec, env in runs:
+        elem = 8 if prec == "double" else 4
+        per_point = 2 * elem if env else 7 * elem  # shared factorisation: RHS in, x out
+        alg = 3 * per_point * edge ** 3
+        row = {"precision": prec, "selectors": env or "default"}
+        for name, app in apps.items():
+            e = dict(os.environ)
+            e.update(env)
+            r = subprocess.run([str(app), str(edge), str(iters), prec], env=e,
+                               capture_output=True, text=True, timeout=300)
+            csv_line = [ln for ln in r.stdout.splitlines() if ln.startswith("CSV,")]
+            if r.returncode != 0 or not csv_line:
+                row[name] = {"error": (r.stderr or r.stdout)[-300:]}
+                continue
+            f = csv_line[-1].split(",")
+            ev_ms = float(f[10])
+            row[name] = {"kernels": [f[2], f[4], f[6]], "iter_ms_wall": float(f[9]),
+                         "iter_ms_events": ev_ms,
+                         "per_direction_ms": [float(f[11]), float(f[12]), float(f[13])],
+                         "gbs": round(alg / (ev_ms * 1e-3) / 1e9, 1)}
+        if "iter_ms_events" in row.get("reference", {}) and \
+                "iter_ms_events" in row.get("b200", {}):
+            row["speedup"] = round(row["reference"]["iter_ms_events"] /
+                                   row["b200"]["iter_ms_events"], 2)
+        out["runs"].append(row)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--configs", default="0,2,3,4")
@@ -390,8 +439,9 @@ def main():
     args = ap.parse_args()
     want = {c.strip() for c in args.configs.split(",")}
     runs = {"0": config0, "2": lambda: config2(args.n2), "3": lambda: config3(args.grids3),
-            "4": lambda: config4(seconds=args.seconds4), "mesh": config_mesh}
-    for c in ("0", "2", "3", "4", "mesh"):
+            "4": lambda: config4(seconds=args.seconds4), "mesh": config_mesh,
+            "refapp": config_refapp}
+    for c in ("0", "2", "3", "4", "mesh", "refapp"):
         if c in want:
             t0 = time.time()
             res = runs[c]()
