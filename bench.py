@@ -373,6 +373,8 @@ def run_ours(args):
             "kernel_family": ran,
             "kernel_variant": variants,
             "per_direction_ms": [round(v, 4) for v in per_dir_ms],
+            "ms_per_iteration": round(ms_step / ITERS, 4),
+            "systems_per_s": round(world * 3 * ITERS * n * n / (ms_step * 1e-3), 1),
             "l2": "no flush: 7 x 128 MiB per axis exceeds the 126 MB L2",
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
         },
