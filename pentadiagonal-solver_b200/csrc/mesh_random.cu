@@ -43,6 +43,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
+#include <type_traits>
 
 #include "pentad_common.hpp"
 #include "pentadsolver_mesh.h"
@@ -61,12 +62,16 @@ constexpr int kMaxCluster = 8;
 constexpr size_t kRingBytes = 2ull * kBatch * sizeof(uint64_t);  // two batches
 static_assert(kBatch % (kPlacers * kMaxCluster) == 0, "placers of a cluster tile a batch");
 
-struct MeshShape {
-  long long inner;   // product of dims below solvedim (row stride)
-  long long n;       // rows per system
-  long long count;   // systems
-  long long per_sys; // draws per system
-  int threads;       // host threads being replayed
+// I is the index type of everything within the grid: int when the grid has
+// fewer than 2^31 points and a system fewer than 2^31 draws, else long long.
+template <typename I> struct MeshShape {
+  I inner;     // product of dims below solvedim (row stride)
+  I n;         // rows per system
+  I count;     // systems
+  I per_sys;   // draws per system
+  I lim_mid;   // 6 n - 15: first draw of row n - 2 (n >= 4)
+  I lim_last;  // 6 n - 10: first draw of row n - 1 (n >= 4)
+  int threads; // host threads being replayed
 };
 
 __device__ __forceinline__ uint64_t mt_mix(uint64_t hi, uint64_t lo, uint64_t far) {
@@ -92,11 +97,11 @@ template <> __device__ __forceinline__ float canonical<float>(uint64_t v) {
 }
 
 // Draws in rows [0, r) of a system of n rows.
-__device__ __forceinline__ long long draws_before(long long r, long long n) {
-  const long long ds = r > 2 ? r - 2 : 0;
-  const long long dl = r > 1 ? r - 1 : 0;
-  const long long du = r < n - 1 ? r : n - 1;
-  const long long dw = n >= 2 ? (r < n - 2 ? r : n - 2) : r;
+template <typename I> __device__ __forceinline__ I draws_before(I r, I n) {
+  const I ds = r > 2 ? r - 2 : 0;
+  const I dl = r > 1 ? r - 1 : 0;
+  const I du = r < n - 1 ? r : n - 1;
+  const I dw = n >= 2 ? (r < n - 2 ? r : n - 2) : r;
   return 2 * r + ds + dl + du + dw;
 }
 
@@ -114,45 +119,46 @@ template <typename F> struct MeshOut {
 // Where draw e of a system falls: its row r and k, the draw's rank in the row.
 // For n >= 4 the rows have 4, 5, 6, ..., 6, 5, 4 draws (row r >= 2 starts at
 // draw 6r - 3 up to row n-2); shorter systems search the prefix counts.
-__device__ __forceinline__ void row_of(long long e, long long n, long long &r, int &k) {
-  if (n >= 4) {
+template <typename I>
+__device__ __forceinline__ void row_of(const MeshShape<I> &s, I e, I &r, int &k) {
+  using U = typename std::make_unsigned<I>::type;
+  if (s.n >= 4) {
     if (e < 4) {
       r = 0;
       k = static_cast<int>(e);
     } else if (e < 9) {
       r = 1;
       k = static_cast<int>(e - 4);
-    } else if (e < 6 * n - 15) {
-      const unsigned long long q = static_cast<unsigned long long>(e + 3) / 6ull;
-      r = static_cast<long long>(q);
+    } else if (e < s.lim_mid) {
+      r = static_cast<I>(static_cast<U>(e + 3) / U(6));
       k = static_cast<int>(e + 3 - 6 * r);
-    } else if (e < 6 * n - 10) {
-      r = n - 2;
-      k = static_cast<int>(e - (6 * n - 15));
+    } else if (e < s.lim_last) {
+      r = s.n - 2;
+      k = static_cast<int>(e - s.lim_mid);
     } else {
-      r = n - 1;
-      k = static_cast<int>(e - (6 * n - 10));
+      r = s.n - 1;
+      k = static_cast<int>(e - s.lim_last);
     }
     return;
   }
-  long long a = 0, b = n;  // the largest a with draws_before(a) <= e
+  I a = 0, b = s.n;  // the largest a with draws_before(a) <= e
   while (b - a > 1) {
-    const long long mid = (a + b) >> 1;
-    if (draws_before(mid, n) <= e) a = mid; else b = mid;
+    const I mid = (a + b) >> 1;
+    if (draws_before<I>(mid, s.n) <= e) a = mid; else b = mid;
   }
   r = a;
-  k = static_cast<int>(e - draws_before(a, n));
+  k = static_cast<int>(e - draws_before<I>(a, s.n));
 }
 
 // A lane's position in its host thread's stream: draw e of system `sys`, whose
 // first element is `start` (= i * inner * n + j for sys = i * inner + j).
-struct Cursor {
-  long long sys, e, j, start;
+template <typename I> struct Cursor {
+  I sys, e, j, start;
 };
 
-__device__ __forceinline__ void cursor_set(Cursor &c, const MeshShape &s, long long sys,
-                                           long long e) {
-  const long long i = sys / s.inner;
+template <typename I>
+__device__ __forceinline__ void cursor_set(Cursor<I> &c, const MeshShape<I> &s, I sys, I e) {
+  const I i = sys / s.inner;
   c.sys = sys;
   c.e = e;
   c.j = sys - i * s.inner;
@@ -160,7 +166,8 @@ __device__ __forceinline__ void cursor_set(Cursor &c, const MeshShape &s, long l
 }
 
 // Moves the cursor `step` draws on; one system ahead at most without a division.
-__device__ __forceinline__ void cursor_advance(Cursor &c, const MeshShape &s, long long step) {
+template <typename I>
+__device__ __forceinline__ void cursor_advance(Cursor<I> &c, const MeshShape<I> &s, I step) {
   c.e += step;
   if (c.e < s.per_sys) return;
   if (c.e - s.per_sys < s.per_sys) {
@@ -173,17 +180,17 @@ __device__ __forceinline__ void cursor_advance(Cursor &c, const MeshShape &s, lo
     }
     return;
   }
-  const long long w = c.e / s.per_sys;
-  cursor_set(c, s, c.sys + w, c.e - w * s.per_sys);
+  const I w = c.e / s.per_sys;
+  cursor_set<I>(c, s, c.sys + w, c.e - w * s.per_sys);
 }
 
 // Stores the draw under cursor c, value v.
-template <typename F>
-__device__ __forceinline__ void place(const MeshShape &s, const Cursor &c, F v,
+template <typename F, typename I>
+__device__ __forceinline__ void place(const MeshShape<I> &s, const Cursor<I> &c, F v,
                                       const MeshOut<F> &out) {
-  long long r;
+  I r;
   int k;
-  row_of(c.e, s.n, r, k);
+  row_of<I>(s, c.e, r, k);
   const bool has[6] = {r > 1, r > 0, true, r < s.n - 1,
                        s.n >= 2 ? r < s.n - 2 : true, true};
   int slot = 0;
@@ -191,7 +198,7 @@ __device__ __forceinline__ void place(const MeshShape &s, const Cursor &c, F v,
     seen += has[slot] ? 1 : 0;
     if (seen == k) break;
   }
-  const long long idx = c.start + r * s.inner;
+  const I idx = c.start + r * s.inner;
   out.pick(slot)[idx] = slot == 2 ? F(6) * v : (slot == 5 ? v : -v);
   if (slot == 2) {
     // the row's entries that take no draw, written once per row
@@ -261,24 +268,24 @@ __device__ __forceinline__ void refill(uint64_t *cur, const uint64_t *prev_last,
 // over distributed shared memory: placing thread p = rank * 624 + lane takes
 // batch draws p, p + 624 C, ... (16 / C of them), so its draws in the stream
 // are 624 C apart.  One cluster barrier per batch.
-template <typename F>
+template <typename F, typename I>
 __global__ void __launch_bounds__(kMeshThreads, 1)
-mesh_random_kernel(MeshShape s, F *ds, F *dl, F *d, F *du, F *dw, F *x) {
+mesh_random_kernel(MeshShape<I> s, F *ds, F *dl, F *d, F *du, F *dw, F *x) {
   extern __shared__ __align__(16) uint64_t ring[];  // [2][kSteps][312], first CTA only
   const MeshOut<F> out{{ds, dl, d, du, dw, x}};
   const unsigned rank = cluster_rank(), csize = cluster_size();
   const long long t = blockIdx.x / csize;
-  const long long q = s.count / s.threads, rem = s.count % s.threads;
+  const long long q = (long long)s.count / s.threads, rem = (long long)s.count % s.threads;
   const long long lo = q * t + (t < rem ? t : rem);
-  const long long total = (q + (t < rem ? 1 : 0)) * s.per_sys;
+  const long long total = (q + (t < rem ? 1 : 0)) * (long long)s.per_sys;
   if (total == 0) return;  // the whole cluster (same t) leaves
   const int warp = threadIdx.x / 32;
   const bool refiller = rank == 0 && warp >= kPlaceWarps;
   const int rk = threadIdx.x - 32 * kPlaceWarps;  // lane within the refilling warps
   const int p_local = threadIdx.x;                // placing thread within the CTA
-  const long long stride = (long long)kPlacers * csize;
-  const int per_batch = kBatch / (int)stride;     // draws per placing thread per batch
-  const long long p = (long long)rank * kPlacers + p_local;
+  const int stride = kPlacers * (int)csize;
+  const int per_batch = kBatch / stride;          // draws per placing thread per batch
+  const int p = (int)rank * kPlacers + p_local;
 
   if (refiller) {
     // seed into the last step of buffer 1, then batch 0 into buffer 0
@@ -294,8 +301,8 @@ mesh_random_kernel(MeshShape s, F *ds, F *dl, F *d, F *du, F *dw, F *x) {
     refill_sync();
     refill(ring, seed, rk);
   }
-  Cursor c;
-  if (p_local < kPlacers) cursor_set(c, s, lo + p / s.per_sys, p % s.per_sys);
+  Cursor<I> c;
+  if (p_local < kPlacers) cursor_set<I>(c, s, (I)lo + (I)p / s.per_sys, (I)p % s.per_sys);
   uint32_t ring0;  // the ring in the first CTA's shared memory
   asm volatile("mapa.shared::cluster.u32 %0, %1, 0;"
                : "=r"(ring0) : "r"((uint32_t)__cvta_generic_to_shared(ring)));
@@ -308,13 +315,12 @@ mesh_random_kernel(MeshShape s, F *ds, F *dl, F *d, F *du, F *dw, F *x) {
       refill(ring + (buf ^ 1) * kBatch, ring + buf * kBatch + (kSteps - 1) * kMtN, rk);
     if (p_local < kPlacers) {
       for (int i = 0; i < per_batch; ++i) {
-        const long long j = p + stride * i;  // draw within the batch
-        const long long g = base + j;
-        if (g < total) {
+        const int j = p + stride * i;  // draw within the batch
+        if (base + j < total) {
           const uint64_t w = ld_cluster_u64(ring0 + (uint32_t)((buf * kBatch + j) * 8));
-          place<F>(s, c, canonical<F>(mt_temper(w)), out);
+          place<F, I>(s, c, canonical<F>(mt_temper(w)), out);
         }
-        cursor_advance(c, s, stride);
+        cursor_advance<I>(c, s, (I)stride);
       }
     }
     cluster_sync_all(refiller);  // batch placed and the next one refilled
@@ -323,19 +329,19 @@ mesh_random_kernel(MeshShape s, F *ds, F *dl, F *d, F *du, F *dw, F *x) {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-// [FP32, FP64][device][cluster width 1, 2, 4, 8]: clusters the device can hold
-// at once (0 = not yet known, -1 = cannot launch)
-int g_active[2][kMaxDevices][4] = {};
+// [FP32, FP64][32-bit, 64-bit indices][device][cluster width 1, 2, 4, 8]:
+// clusters the device can hold at once (0 = not yet known, -1 = cannot launch)
+int g_active[2][2][kMaxDevices][4] = {};
 
 // How many clusters of `width` CTAs the device runs at once, found once per
 // device, precision and width (clusters of 8 CTAs need 8 free SMs of one GPC,
 // so fewer fit than SMs / 8).
-template <typename F> int active_clusters(int dev, int width) {
+template <typename F, typename I> int active_clusters(int dev, int width) {
   std::lock_guard<std::mutex> lock(g_mu);
-  int &a = g_active[sizeof(F) == 8][dev][width == 8 ? 3 : width / 2];
+  int &a = g_active[sizeof(F) == 8][sizeof(I) == 8][dev][width == 8 ? 3 : width / 2];
   if (a != 0) return a;
   a = -1;
-  auto kern = mesh_random_kernel<F>;
+  auto kern = mesh_random_kernel<F, I>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)kRingBytes) != cudaSuccess) {
     cudaGetLastError();
@@ -359,42 +365,24 @@ template <typename F> int active_clusters(int dev, int width) {
   return a;
 }
 
-template <typename F>
-pentadStatus_t mesh_random(const int *dims, int ndims, int solvedim, int n_threads, F *ds,
-                           F *dl, F *d, F *du, F *dw, F *x, void *stream) {
-  if (dims == nullptr || ndims < 1 || ndims > PENTAD_MAXDIM || solvedim < 0 ||
-      solvedim >= ndims || n_threads < 1 || n_threads > PENTADSOLVER_MESH_MAX_THREADS)
-    return PENTAD_STATUS_INVALID_VALUE;
-  if (!ds || !dl || !d || !du || !dw || !x) return PENTAD_STATUS_INVALID_VALUE;
-  MeshShape s{1, dims[solvedim], 1, 0, n_threads};
-  for (int k = 0; k < ndims; ++k) {
-    if (dims[k] < 1) return PENTAD_STATUS_INVALID_VALUE;
-    if (k < solvedim) s.inner *= dims[k];
-    if (k != solvedim) s.count *= dims[k];
-  }
-  // draws per system: rows 0..n-1 in full
-  {
-    const long long n = s.n, r = n;
-    const long long dsn = r > 2 ? r - 2 : 0, dln = r > 1 ? r - 1 : 0;
-    const long long dun = r < n - 1 ? r : n - 1;
-    const long long dwn = n >= 2 ? (r < n - 2 ? r : n - 2) : r;
-    s.per_sys = 2 * r + dsn + dln + dun + dwn;
-  }
+template <typename F, typename I>
+pentadStatus_t launch_mesh(const MeshShape<I> &s, int n_threads, F *ds, F *dl, F *d, F *du,
+                           F *dw, F *x, void *stream) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     cudaGetLastError();
     return PENTAD_STATUS_NOT_INITIALIZED;
   }
-  auto kern = mesh_random_kernel<F>;
+  auto kern = mesh_random_kernel<F, I>;
   // CTAs per host thread: the widest cluster (8, 4, 2) of which the device
   // holds one per host thread at once; else one CTA per host thread
   int csize = 1;
   for (int w = kMaxCluster; w > 1; w /= 2)
-    if (active_clusters<F>(dev, w) >= n_threads) {
+    if (active_clusters<F, I>(dev, w) >= n_threads) {
       csize = w;
       break;
     }
-  if (csize == 1 && active_clusters<F>(dev, 1) < 1) return PENTAD_STATUS_EXECUTION_FAILED;
+  if (csize == 1 && active_clusters<F, I>(dev, 1) < 1) return PENTAD_STATUS_EXECUTION_FAILED;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(n_threads * csize));
   cfg.blockDim = dim3(kMeshThreads);
@@ -413,6 +401,33 @@ pentadStatus_t mesh_random(const int *dims, int ndims, int solvedim, int n_threa
     return PENTAD_STATUS_EXECUTION_FAILED;
   }
   return PENTAD_STATUS_SUCCESS;
+}
+
+template <typename F>
+pentadStatus_t mesh_random(const int *dims, int ndims, int solvedim, int n_threads, F *ds,
+                           F *dl, F *d, F *du, F *dw, F *x, void *stream) {
+  if (dims == nullptr || ndims < 1 || ndims > PENTAD_MAXDIM || solvedim < 0 ||
+      solvedim >= ndims || n_threads < 1 || n_threads > PENTADSOLVER_MESH_MAX_THREADS)
+    return PENTAD_STATUS_INVALID_VALUE;
+  if (!ds || !dl || !d || !du || !dw || !x) return PENTAD_STATUS_INVALID_VALUE;
+  long long inner = 1, count = 1, points = 1;
+  const long long n = dims[solvedim];
+  for (int k = 0; k < ndims; ++k) {
+    if (dims[k] < 1) return PENTAD_STATUS_INVALID_VALUE;
+    if (k < solvedim) inner *= dims[k];
+    if (k != solvedim) count *= dims[k];
+    points *= dims[k];
+  }
+  // draws per system: rows 0..n-1 in full
+  const long long per_sys = 2 * n + (n > 2 ? n - 2 : 0) + (n > 1 ? n - 1 : 0) + (n - 1) +
+                            (n >= 2 ? n - 2 : n);
+  if (points < (1LL << 31) && per_sys < (1LL << 31)) {
+    const MeshShape<int> s{(int)inner, (int)n, (int)count, (int)per_sys,
+                           (int)(6 * n - 15), (int)(6 * n - 10), n_threads};
+    return launch_mesh<F, int>(s, n_threads, ds, dl, d, du, dw, x, stream);
+  }
+  const MeshShape<long long> s{inner, n, count, per_sys, 6 * n - 15, 6 * n - 10, n_threads};
+  return launch_mesh<F, long long>(s, n_threads, ds, dl, d, du, dw, x, stream);
 }
 
 }  // namespace
