@@ -1034,6 +1034,23 @@ bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf, int &
   return true;
 }
 
+// CTAs for a strided launch with dw2 in the buffer (factor mode 1): each lane
+// quarter keeps about one tile of (dw2, x2) pairs live in L2 (written by the
+// forward sweep, read back by the substitution), and once all quarters' live
+// scratch outgrows about 50 MB -- 40% of the L2, the rest holding the streamed
+// arrays -- it spills to HBM (at 512^3 FP64 the x solve moves 1.36x its
+// algorithmic bytes).  At 512^3 FP64 (131 KB a tile) 96 CTAs beat 148 by 5-7%
+// along y and z, 74 lose 13%; along x, whose loads keep normal L2 priority, the
+// full grid stays best.  Factor mode 2 keeps the full grid (not measured).
+template <typename F>
+int scratch_grid_cap(const SolveArgs<F> &a, const TmemConfig &c, int sm_count) {
+  if (c.contig || c.fmode != 1) return sm_count;
+  const long long tile_bytes = 2 * split_row<F>(a.L, false) * TS * 2 * (long long)sizeof(F);
+  const long long cap = (50ll << 20) / (NCONS * tile_bytes);
+  const int floor_ctas = 2 * sm_count / 3;
+  return cap >= sm_count ? sm_count : (cap < floor_ctas ? floor_ctas : (int)cap);
+}
+
 template <typename F>
 cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count,
                         cudaStream_t stream) {
@@ -1041,6 +1058,7 @@ cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count
   if (!fill_job<F>(J, a, c.contig, static_cast<F *>(a.scratch), 0))
     return cudaErrorInvalidValue;
   const int flags = ((reinterpret_cast<uintptr_t>(a.scratch) % 128 == 0) ? 1 : 0);
+  sm_count = scratch_grid_cap<F>(a, c, sm_count);
 #define PENTA_X(FT_, C_, W_, ST_, XST_)                                                   \
   if (std::is_same<F, FT_>::value && c.contig == C_ && c.fmode == W_ && c.stages == ST_ &&  \
       c.xstages == XST_)                                                                  \
