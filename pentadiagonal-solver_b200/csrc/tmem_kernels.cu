@@ -247,7 +247,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   if (role == 1) {
     // read once: evict first -- except along x with dw2 in the buffer, where
     // the larger scratch round trip does better against normal-priority loads
-    const uint64_t pol_in = (CONTIG && FM >= 1) ? l2_policy_normal() : l2_policy_first();
+    const uint64_t pol_in = (CONTIG && FM == 2) ? l2_policy_normal() : l2_policy_first();
     int slot = 0, use = 0, cursor = 0, fenced = -1;
     Geo JG;
     load_geo(job_of(gw, cursor), JG);
@@ -1034,19 +1034,21 @@ bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf, int &
   return true;
 }
 
-// CTAs for a strided launch with dw2 in the buffer (factor mode 1): each lane
-// quarter keeps about one tile of (dw2, x2) pairs live in L2 (written by the
-// forward sweep, read back by the substitution), and once all quarters' live
-// scratch outgrows about 50 MB -- 40% of the L2, the rest holding the streamed
-// arrays -- it spills to HBM (at 512^3 FP64 the x solve moves 1.36x its
-// algorithmic bytes).  At 512^3 FP64 (131 KB a tile) 96 CTAs beat 148 by 5-7%
-// along y and z, 74 lose 13%; along x, whose loads keep normal L2 priority, the
-// full grid stays best.  Factor mode 2 keeps the full grid (not measured).
+// CTAs for a launch with dw2 in the buffer (factor mode 1): each lane quarter
+// keeps about one tile of (dw2, x2) pairs live in L2 (written by the forward
+// sweep, read back by the substitution), and once all quarters' live scratch
+// outgrows about half the L2 -- the rest holding the streamed arrays -- it
+// spills to HBM (at 512^3 FP64 the x solve moved 1.36x its algorithmic bytes
+// with all 148 SMs).  At 512^3 FP64 (131 KB a tile) 96 CTAs beat 148 by 5-7%
+// along y and z (74 lose 13%); along x, with evict-first loads, 111 CTAs beat
+// 148 by 5%.  Factor mode 2 keeps the full grid (n = 1024: no gain measured).
 template <typename F>
 int scratch_grid_cap(const SolveArgs<F> &a, const TmemConfig &c, int sm_count) {
-  if (c.contig || c.fmode != 1) return sm_count;
-  const long long tile_bytes = 2 * split_row<F>(a.L, false) * TS * 2 * (long long)sizeof(F);
-  const long long cap = (50ll << 20) / (NCONS * tile_bytes);
+  if (c.fmode != 1) return sm_count;
+  const long long tile_bytes =
+      2 * split_row<F>(a.L, c.contig) * TS * 2 * (long long)sizeof(F);
+  const long long budget = c.contig ? (58ll << 20) : (50ll << 20);
+  const long long cap = budget / (NCONS * tile_bytes);
   const int floor_ctas = 2 * sm_count / 3;
   return cap >= sm_count ? sm_count : (cap < floor_ctas ? floor_ctas : (int)cap);
 }
