@@ -488,7 +488,9 @@ def cpu_solver():
             "port", "oracle/penta_oracle.c")
 
 
-def cpu_baseline(n, budget_s=12.0, max_iters=50):
+def cpu_baseline(n, budget_s=12.0, max_iters=1000):
+    """The reference's CPU solver on the host cores for about budget_s seconds
+    of whole ADI iterations (the bounded sample the line reports)."""
     from oracle import oracle
 
     threads = _cpu_threads()
