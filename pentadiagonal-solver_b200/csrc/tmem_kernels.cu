@@ -247,7 +247,10 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   if (role == 1) {
     // read once: evict first -- except along x with dw2 in the buffer, where
     // the larger scratch round trip does better against normal-priority loads
-    const uint64_t pol_in = (CONTIG && FM == 2) ? l2_policy_normal() : l2_policy_first();
+    // streamed loads evict-first, except along x with factors in the buffer, where
+    // they keep normal priority unless the launch capped its CTAs (flags bit 1)
+    const uint64_t pol_in = (CONTIG && FM >= 1 && !(flags & 2)) ? l2_policy_normal()
+                                                                 : l2_policy_first();
     int slot = 0, use = 0, cursor = 0, fenced = -1;
     Geo JG;
     load_geo(job_of(gw, cursor), JG);
@@ -1034,17 +1037,21 @@ bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf, int &
   return true;
 }
 
-// CTAs for a launch with dw2 in the buffer (factor mode 1): each lane quarter
-// keeps about one tile of (dw2, x2) pairs live in L2 (written by the forward
-// sweep, read back by the substitution), and once all quarters' live scratch
-// outgrows about half the L2 -- the rest holding the streamed arrays -- it
-// spills to HBM (at 512^3 FP64 the x solve moved 1.36x its algorithmic bytes
-// with all 148 SMs).  At 512^3 FP64 (131 KB a tile) 96 CTAs beat 148 by 5-7%
-// along y and z (74 lose 13%); along x, with evict-first loads, 111 CTAs beat
-// 148 by 5%.  Factor mode 2 keeps the full grid (n = 1024: no gain measured).
+// CTAs for an FP64 launch with dw2 in the buffer (factor mode 1) and many tiles
+// per lane quarter: each quarter keeps about one tile of (dw2, x2) pairs live in
+// L2 (written by the forward sweep, read back by the substitution), and once all
+// quarters' live scratch outgrows about half the L2 -- the rest holding the
+// streamed arrays -- it spills to HBM (at 512^3 FP64 the x solve moved 1.36x its
+// algorithmic bytes with all 148 SMs).  At 512^3 FP64 (131 KB a tile, 28 tiles
+// a quarter) 96 CTAs beat 148 by 5-7% along y and z (74 lose 13%); along x,
+// with evict-first loads, 111 CTAs beat 148 by 5%.  With few tiles a quarter the
+// lost parallelism costs more than the spill (FP32 1024 x 128 x 128, under two
+// tiles a quarter: 20-40% slower capped), so the cap needs 8 tiles a quarter;
+// FP32 and factor mode 2 (n = 1024 FP64: no gain) keep the full grid.
 template <typename F>
-int scratch_grid_cap(const SolveArgs<F> &a, const TmemConfig &c, int sm_count) {
-  if (c.fmode != 1) return sm_count;
+int scratch_grid_cap(const SolveArgs<F> &a, const TmemConfig &c, long long tiles,
+                     int sm_count) {
+  if (sizeof(F) != 8 || c.fmode != 1 || tiles < 8LL * NCONS * sm_count) return sm_count;
   const long long tile_bytes =
       2 * split_row<F>(a.L, c.contig) * TS * 2 * (long long)sizeof(F);
   const long long budget = c.contig ? (58ll << 20) : (50ll << 20);
@@ -1059,8 +1066,10 @@ cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count
   TmemJob<F> J;
   if (!fill_job<F>(J, a, c.contig, static_cast<F *>(a.scratch), 0))
     return cudaErrorInvalidValue;
-  const int flags = ((reinterpret_cast<uintptr_t>(a.scratch) % 128 == 0) ? 1 : 0);
-  sm_count = scratch_grid_cap<F>(a, c, sm_count);
+  int flags = ((reinterpret_cast<uintptr_t>(a.scratch) % 128 == 0) ? 1 : 0);
+  const int capped = scratch_grid_cap<F>(a, c, J.n_tiles, sm_count);
+  if (capped < sm_count) flags |= 2;  // capped: streamed loads evict-first
+  sm_count = capped;
 #define PENTA_X(FT_, C_, W_, ST_, XST_)                                                   \
   if (std::is_same<F, FT_>::value && c.contig == C_ && c.fmode == W_ && c.stages == ST_ &&  \
       c.xstages == XST_)                                                                  \
