@@ -75,8 +75,7 @@ def reference_text(fx: dict) -> str:
     return "\n".join(lines) + "\n"
 
 
-FIXTURE_CASES = [(fam, k) for fam, nd in fixtures.FAMILIES.items() for k in range(nd)
-                 if not fam.endswith("large") or fam == "two_dim_large"]
+FIXTURE_CASES = [(fam, k) for fam, nd in fixtures.FAMILIES.items() for k in range(nd)]
 
 
 @pytest.mark.parametrize("fam,solvedim", FIXTURE_CASES)
