@@ -1068,7 +1068,9 @@ cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count
     return cudaErrorInvalidValue;
   int flags = ((reinterpret_cast<uintptr_t>(a.scratch) % 128 == 0) ? 1 : 0);
   const int capped = scratch_grid_cap<F>(a, c, J.n_tiles, sm_count);
-  if (capped < sm_count) flags |= 2;  // capped: streamed loads evict-first
+  // streamed loads evict-first when the grid is capped, and for FP32 along x with
+  // dw2 in the buffer (1024 x 128 x 128: 118 against 129 us with normal priority)
+  if (capped < sm_count || (sizeof(F) == 4 && c.contig && c.fmode == 1)) flags |= 2;
   sm_count = capped;
 #define PENTA_X(FT_, C_, W_, ST_, XST_)                                                   \
   if (std::is_same<F, FT_>::value && c.contig == C_ && c.fmode == W_ && c.stages == ST_ &&  \
