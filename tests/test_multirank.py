@@ -66,3 +66,27 @@ def test_reference_arm_prints_on_rank_zero_only():
                         "--gpus", "2"], env=env, capture_output=True, text=True, timeout=120)
     assert p.returncode == 0, p.stderr
     assert p.stdout.strip() == ""
+
+
+def test_reference_arm_line_carries_the_contract_keys():
+    p = subprocess.run([sys.executable, str(REPO / "bench.py"), "--impl", "reference",
+                        "--steps", "3", "--warmup", "3", "--n", "64"],
+                       capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    line = json.loads(p.stdout.strip().splitlines()[-1])
+    sys.path.insert(0, str(REPO))
+    import bench
+
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+              "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
+              "cpu_baseline", "e2e"):
+        assert k in line, k
+    assert line["impl"] == "reference" and line["metric"] == bench.METRIC
+    assert line["unit"] == "GB/s" and line["higher_is_better"] is True and line["value"] > 0
+    assert line["steps"] == 3 and line["warmup"] == 3 and line["n_gpus"] == 1
+    cb = line["cpu_baseline"]
+    assert cb["value"] == line["value"] and cb["kind"] in ("reference", "port")
+    assert cb["cores"] >= 1 and cb["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": "GB/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+    assert line["config"]["workload"] == "adi_256cube_fp64_general_50iter"
