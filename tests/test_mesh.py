@@ -232,3 +232,18 @@ def test_mesh_random_rejects_bad_arguments_without_a_device():
     bad = (ctypes.c_int * 3)(8, 0, 8)
     assert f(bad, 3, 0, 4, *fake, None) == ps.INVALID_VALUE
     assert f(dims, 3, 0, 4, None, *fake[1:], None) == ps.INVALID_VALUE
+
+
+@pytest.mark.parametrize("shape", [(7,), (2, 1, 3, 1, 2, 1, 2, 2)])
+@pytest.mark.parametrize("fmt", ["text", "binary"])
+def test_round_trip_any_rank(tmp_path, shape, fmt):
+    arrs = random_arrays(shape, np.float64, 11)
+    code = mesh.TEXT if fmt == "text" else mesh.BINARY_F64
+    path = tmp_path / "grid.fx"
+    mesh.write_fixture(path, arrs, solvedim=len(shape) - 1, fmt=code)
+    info = mesh.fixture_info(path)
+    assert info["ndims"] == len(shape) and info["dims"] == list(reversed(shape))
+    assert info["solvedim"] == len(shape) - 1 and info["format"] == code
+    back = mesh.read_fixture(path, np.float64)
+    for k in ("ds", "dl", "d", "du", "dw", "x", "u"):
+        assert same_bits(back[k], arrs[k]), k
