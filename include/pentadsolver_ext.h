@@ -38,11 +38,27 @@ EXTERN_C PENTAD_API pentadStatus_t pentadsolver_S_gpsv_batch_ex(
     const int *t_dims, int t_ndim, int t_solvedim, void *t_buffer,
     size_t t_buffer_bytes, void *stream);
 
-/* Synchronise `stream`, then read and clear the device status bits raised by
- * the solves issued so far on the current device (bit 0: a pivot was zero or
- * not finite).  Returns PENTAD_STATUS_ZERO_PIVOT when bit 0 was set. */
+/* Read and clear the status bits raised by this handle's solves (bit 0: a
+ * pivot was zero or not finite; bit 1: a wait inside a kernel ran out), then
+ * synchronise `stream`.  The read and the clear are one atomic exchange on the
+ * device, issued on `stream`: a bit raised by a kernel on another stream is
+ * either returned now or kept for the next check.  Every created handle has a
+ * status word of its own (a slot of a fixed device array, so nothing is
+ * allocated); the NULL handle's word is shared by all handle-less calls on
+ * the device, and so is it for handles created after the array's 4095 slots
+ * are taken.  Returns PENTAD_STATUS_ZERO_PIVOT when bit 0 was set, and
+ * PENTAD_STATUS_INVALID_VALUE when the handle is bound to another device
+ * than the current one. */
 EXTERN_C PENTAD_API pentadStatus_t pentadsolver_status_check(pentadsolver_handle_t handle,
                                                   void *stream, int *bits);
+
+/* Test of the bounded waits every kernel uses: launches on `stream` a kernel
+ * whose one mbarrier wait can never complete; the wait gives up after
+ * `limit_us` microseconds (1 .. 1,000,000) and raises bit 1 in the handle's
+ * status word, as a solve does when one of its waits runs out.  The device
+ * stays usable; pentadsolver_status_check then reports the bit. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_selftest_bounded_wait(
+    pentadsolver_handle_t handle, unsigned limit_us, void *stream);
 
 /* Per-handle algorithm choice for one direction (0 = x, 1 = middle, 2 =
  * outermost): "naive", "transpose", "thomas-pcr", "shared-fact", "auto", or
@@ -110,6 +126,10 @@ EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_create_split(
 EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_execute(pentadsolver_plan_t plan,
                                                               void *stream);
 EXTERN_C PENTAD_API const char *pentadsolver_plan_describe(pentadsolver_plan_t plan);
+/* As pentadsolver_status_check, for the kernels of this plan's executes: every
+ * plan reports into a status word of its own. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_status_check(pentadsolver_plan_t plan,
+                                                                  void *stream, int *bits);
 EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_destroy(pentadsolver_plan_t plan);
 
 /* ---- Mixed precision: FP32 sweeps, FP64 residual and correction -----------
@@ -161,7 +181,9 @@ EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_estimates(pentadsolver_plan
  *     (cudaGetSymbolAddress) with that device current, so make that first
  *     call before any stream capture on the device.
  * Asynchronous on `stream` (a cudaStream_t, or NULL for the legacy default
- * stream); arguments otherwise as pentadsolver_D_gpsv_batch. */
+ * stream).  `handle` (NULL: the current device's default context) receives
+ * the status bits, read by pentadsolver_status_check; arguments and shape
+ * rules otherwise as pentadsolver_D_gpsv_batch. */
 #define PENTADSOLVER_NOALLOC_MAX_BYTES (16u * 1024u * 1024u)
 EXTERN_C PENTAD_API pentadStatus_t pentadsolver_D_gpsv_batch_noalloc(
     pentadsolver_handle_t handle, const double *ds, const double *dl,

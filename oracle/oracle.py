@@ -32,6 +32,18 @@ REF_ORIG_SO = HERE / "_ref" / "libpentad_orig_ref.so"
 REF_SIMD_SO = HERE / "_ref" / "libpentad_simd_ref.so"
 REF_CUDA_SO = HERE / "_ref" / "libpentad_cuda_ref.so"
 
+#: Environment variable naming the reference source tree (read by the build
+#: recipe, the fixture generator and the fixture tests); unset, the tree is
+#: looked for at the path below.
+REFERENCE_ENV = "PENTA_REFERENCE_DIR"
+REFERENCE_DEFAULT = "/root/reference"
+
+
+def reference_dir() -> Path:
+    """Where the reference's sources are (they may be absent)."""
+    return Path(os.environ.get(REFERENCE_ENV) or REFERENCE_DEFAULT)
+
+
 _P = ctypes.c_void_p
 _libs: dict[str, ctypes.CDLL] = {}
 

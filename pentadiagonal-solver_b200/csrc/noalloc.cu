@@ -67,23 +67,16 @@ cudaError_t scratch_address(double **out) {
 }  // namespace
 
 extern "C" PENTAD_API pentadStatus_t pentadsolver_D_gpsv_batch_noalloc(
-    pentadsolver_handle_t /*handle*/, const double *ds, const double *dl,
+    pentadsolver_handle_t handle, const double *ds, const double *dl,
     const double *d, const double *du, const double *dw, double *x,
     const int *t_dims, int t_ndim, int t_solvedim, void *stream) {
-  // Shape checks first: nothing touches the device for a rejected call.
-  if (t_dims == nullptr || t_ndim < 1 || t_ndim > PENTAD_MAXDIM ||
-      t_solvedim < 0 || t_solvedim >= t_ndim)
-    return PENTAD_STATUS_INVALID_VALUE;
+  // Shape checks first (the same rules as every other entry point):
+  // nothing touches the device for a rejected call.
+  penta::Lines L{};
+  const char *why = "";
+  pentadStatus_t st = penta::check_shape(t_dims, t_ndim, t_solvedim, L, &why);
+  if (st != PENTAD_STATUS_SUCCESS) return st;
   if (!ds || !dl || !d || !du || !dw || !x) return PENTAD_STATUS_INVALID_VALUE;
-  long long inner = 1, outer = 1;
-  for (int k = 0; k < t_ndim; ++k) {
-    if (t_dims[k] < 1) return PENTAD_STATUS_INVALID_VALUE;
-    if (k < t_solvedim) inner *= t_dims[k];
-    if (k > t_solvedim) outer *= t_dims[k];
-  }
-  const long long n = t_dims[t_solvedim];
-  if (n <= 4) return PENTAD_STATUS_INVALID_VALUE;  // as every other entry point
-  penta::Lines L{n, inner, inner * outer};
   const size_t need = penta::thomas_global_scratch<double>(L);
   if (need > kNoallocBytes) {
     std::fprintf(stderr,
@@ -95,15 +88,16 @@ extern "C" PENTAD_API pentadStatus_t pentadsolver_D_gpsv_batch_noalloc(
     return PENTAD_STATUS_INVALID_VALUE;
   }
 
+  // the handle (NULL: the current device's default context) gives the status
+  // word, as for pentadsolver_D_gpsv_batch_ex
+  int *status_word = nullptr;
+  st = penta::bind_handle(handle, &status_word, &why);
+  if (st != PENTAD_STATUS_SUCCESS) return st;
   double *scratch = nullptr;
   if (scratch_address(&scratch) != cudaSuccess) {
     cudaGetLastError();
     return PENTAD_STATUS_NOT_INITIALIZED;
   }
-  int dev = 0;
-  cudaGetDevice(&dev);
-  int *status_word = penta::device_status_word(dev);
-  if (status_word == nullptr) return PENTAD_STATUS_INTERNAL_ERROR;
 
   penta::SolveArgs<double> a{ds, dl, d, du, dw, x, L, scratch, kNoallocBytes,
                              status_word};

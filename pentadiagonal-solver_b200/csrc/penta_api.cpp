@@ -92,6 +92,7 @@ Knobs knobs_from(const std::string &tuning) {
 // ---------------------------------------------------------------------------
 struct Context {
   int device = -1;
+  int slot = 0;  // status word slot (0: shared by the handle-less calls)
   int sm_count = 0;
   int smem_optin = 0;  // max dynamic shared memory per block (bytes)
   std::mutex mu;
@@ -185,11 +186,18 @@ pentadStatus_t make_shape(const int *dims, int ndim, int solvedim, Shape &sh,
     *why = "t_solvedim out of range";
     return PENTAD_STATUS_INVALID_VALUE;
   }
-  long long inner = 1, outer = 1;
+  // products are checked before they are formed: no overflow whatever the dims
+  constexpr long long kMaxSystems = 1LL << 40;
+  long long inner = 1, systems = 1;
   for (int k = 0; k < ndim; ++k) {
     if (dims[k] < 1) { *why = "a dimension is < 1"; return PENTAD_STATUS_INVALID_VALUE; }
+    if (k == solvedim) continue;
+    if (systems > kMaxSystems / dims[k]) {
+      *why = "grid too large";
+      return PENTAD_STATUS_INVALID_VALUE;
+    }
+    systems *= dims[k];
     if (k < solvedim) inner *= dims[k];
-    if (k > solvedim) outer *= dims[k];
   }
   const long long n = dims[solvedim];
   if (n <= 4) {
@@ -197,13 +205,13 @@ pentadStatus_t make_shape(const int *dims, int ndim, int solvedim, Shape &sh,
     *why = "the solve dimension must be longer than 4";
     return PENTAD_STATUS_INVALID_VALUE;
   }
-  if (n > (1LL << 24) || inner * outer > (1LL << 40)) {
+  if (n > (1LL << 24)) {
     *why = "grid too large";
     return PENTAD_STATUS_INVALID_VALUE;
   }
   sh.L.n = n;
   sh.L.inner = inner;
-  sh.L.n_sys = inner * outer;
+  sh.L.n_sys = systems;
   sh.dir = (solvedim == 0) ? 0 : (solvedim == ndim - 1 ? 2 : 1);
   return PENTAD_STATUS_SUCCESS;
 }
@@ -435,11 +443,29 @@ void record(Context &ctx, int dir, const char *family, const std::string &var) {
 // ---------------------------------------------------------------------------
 // The solve
 // ---------------------------------------------------------------------------
+// The context's device must be current: its cached device properties and its
+// status word's address belong to that device.
+bool on_own_device(const Context &ctx, const char **why) {
+  int cur = -1;
+  if (cudaGetDevice(&cur) != cudaSuccess) {
+    cudaGetLastError();
+    *why = "no usable CUDA device";
+    return false;
+  }
+  if (cur != ctx.device) {
+    *why = "the handle is bound to another device than the current one";
+    return false;
+  }
+  return true;
+}
+
+// `slot` >= 0 reports into that status slot instead of the context's own
+// (a plan's grids solved one by one).
 template <typename F>
 pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
                      const F *du, const F *dw, F *x, const int *dims,
                      int ndim, int solvedim, void *buf, size_t buf_bytes,
-                     cudaStream_t stream, const char **why) {
+                     cudaStream_t stream, const char **why, int slot = -1) {
   Shape sh;
   pentadStatus_t st = make_shape(dims, ndim, solvedim, sh, why);
   if (st != PENTAD_STATUS_SUCCESS) return st;
@@ -451,7 +477,8 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
     *why = "no usable CUDA device";
     return PENTAD_STATUS_NOT_INITIALIZED;
   }
-  int *status_word = device_status_word(ctx.device);
+  if (!on_own_device(ctx, why)) return PENTAD_STATUS_INVALID_VALUE;
+  int *status_word = penta::status_word(ctx.device, slot >= 0 ? slot : ctx.slot);
   if (status_word == nullptr) {
     *why = "cannot address the device status word";
     return PENTAD_STATUS_INTERNAL_ERROR;
@@ -658,6 +685,7 @@ struct PlanSingle {  // a grid the batched kernel does not take: solved alone
 
 struct Plan {
   Context *ctx = nullptr;
+  int slot = 0;  // status word slot of this plan
   int elem = 8, solvedim = 0;
   bool contig = false, w2s = false, discard = false;
   unsigned char *table = nullptr, *scratch = nullptr;
@@ -676,7 +704,12 @@ struct Plan {
   double *est = nullptr;         // device [count][2]
   int count = 0;
   Plan *fp32 = nullptr;          // the FP32 plan over the cast copies
-  ~Plan() { delete fp32; }
+  // the slot the plan's kernels report into (a refine plan's FP32 sweeps)
+  int report_slot() const { return fp32 ? fp32->slot : slot; }
+  ~Plan() {
+    delete fp32;
+    if (ctx) status_slot_release(slot, ctx->device);
+  }
 };
 
 // Memory of a plan: a job table (table_bytes) and scratch (scratch_bytes:
@@ -823,6 +856,7 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
   }
   Plan *p = new Plan();
   p->ctx = &ctx;
+  p->slot = status_slot_acquire();
   p->elem = sizeof(F);
   p->solvedim = solvedim;
   p->contig = contig;
@@ -846,7 +880,9 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
 
 template <typename F> pentadStatus_t plan_run(Plan &p, cudaStream_t stream) {
   Context &ctx = *p.ctx;
-  int *status = device_status_word(ctx.device);
+  const char *why = "";
+  if (!on_own_device(ctx, &why)) return PENTAD_STATUS_INVALID_VALUE;
+  int *status = status_word(ctx.device, p.slot);
   if (status == nullptr) return PENTAD_STATUS_INTERNAL_ERROR;
   for (const Plan::Group &g : p.groups) {
     const cudaError_t e =
@@ -858,12 +894,11 @@ template <typename F> pentadStatus_t plan_run(Plan &p, cudaStream_t stream) {
     }
   }
   for (const PlanSingle &s : p.singles) {
-    const char *why = "";
     const pentadStatus_t st =
         solve<F>(ctx, static_cast<const F *>(s.g.ds), static_cast<const F *>(s.g.dl),
                  static_cast<const F *>(s.g.d), static_cast<const F *>(s.g.du),
                  static_cast<const F *>(s.g.dw), static_cast<F *>(s.g.x), s.g.dims, s.g.ndim,
-                 p.solvedim, p.scratch + s.offset, s.bytes, stream, &why);
+                 p.solvedim, p.scratch + s.offset, s.bytes, stream, &why, p.slot);
     if (st != PENTAD_STATUS_SUCCESS) return st;
   }
   return PENTAD_STATUS_SUCCESS;
@@ -996,6 +1031,17 @@ void refine_fp32_grids(int count, const pentadsolver_grid_t *grids,
   }
 }
 
+// Read and clear one status slot; ZERO_PIVOT when bit 0 was set.
+pentadStatus_t take_status(int device, int slot, cudaStream_t stream, int *bits) {
+  int host = 0;
+  if (status_take(device, slot, stream, &host) != cudaSuccess) {
+    cudaGetLastError();
+    return PENTAD_STATUS_EXECUTION_FAILED;
+  }
+  if (bits) *bits = host;
+  return (host & STATUS_ZERO_PIVOT_BIT) ? PENTAD_STATUS_ZERO_PIVOT : PENTAD_STATUS_SUCCESS;
+}
+
 size_t size_query(const int *dims, int ndim, int solvedim, size_t elem) {
   Shape sh;
   const char *why = "";
@@ -1005,6 +1051,29 @@ size_t size_query(const int *dims, int ndim, int solvedim, size_t elem) {
 }
 
 }  // namespace
+
+pentadStatus_t check_shape(const int *dims, int ndim, int solvedim, Lines &L, const char **why) {
+  Shape sh;
+  const pentadStatus_t st = make_shape(dims, ndim, solvedim, sh, why);
+  if (st == PENTAD_STATUS_SUCCESS) L = sh.L;
+  return st;
+}
+
+pentadStatus_t bind_handle(pentadsolver_handle_t h, int **status, const char **why) {
+  Context *ctx = resolve(h);
+  if (!ctx->init()) {
+    *why = "no usable CUDA device";
+    return PENTAD_STATUS_NOT_INITIALIZED;
+  }
+  if (!on_own_device(*ctx, why)) return PENTAD_STATUS_INVALID_VALUE;
+  *status = status_word(ctx->device, ctx->slot);
+  if (*status == nullptr) {
+    *why = "cannot address the device status word";
+    return PENTAD_STATUS_INTERNAL_ERROR;
+  }
+  return PENTAD_STATUS_SUCCESS;
+}
+
 }  // namespace penta
 
 using penta::Context;
@@ -1017,6 +1086,7 @@ extern "C" void pentadsolver_create(pentadsolver_handle_t *handle,
                                     const int * /*num_procs*/) {
   if (handle == nullptr) return;
   auto *c = new Context();
+  c->slot = penta::status_slot_acquire();
   {
     std::lock_guard<std::mutex> lock(penta::g_reg_mu);
     penta::g_live.insert(c);
@@ -1032,7 +1102,10 @@ extern "C" void pentadsolver_destroy(pentadsolver_handle_t *handle) {
     std::lock_guard<std::mutex> lock(penta::g_reg_mu);
     owned = penta::g_live.erase(c) > 0;
   }
-  if (owned) delete c;
+  if (owned) {
+    penta::status_slot_release(c->slot, c->device);
+    delete c;
+  }
   *handle = nullptr;
 }
 
@@ -1173,22 +1246,26 @@ extern "C" pentadStatus_t pentadsolver_status_check(pentadsolver_handle_t h,
                                                     void *stream, int *bits) {
   Context *ctx = penta::resolve(h);
   if (!ctx->init()) return PENTAD_STATUS_NOT_INITIALIZED;
-  int *word = penta::device_status_word(ctx->device);
+  const char *why = "";
+  if (!penta::on_own_device(*ctx, &why)) return PENTAD_STATUS_INVALID_VALUE;
+  return penta::take_status(ctx->device, ctx->slot, static_cast<cudaStream_t>(stream), bits);
+}
+
+extern "C" pentadStatus_t pentadsolver_selftest_bounded_wait(pentadsolver_handle_t h,
+                                                             unsigned limit_us, void *stream) {
+  if (limit_us == 0 || limit_us > 1000000u) return PENTAD_STATUS_INVALID_VALUE;
+  Context *ctx = penta::resolve(h);
+  if (!ctx->init()) return PENTAD_STATUS_NOT_INITIALIZED;
+  const char *why = "";
+  if (!penta::on_own_device(*ctx, &why)) return PENTAD_STATUS_INVALID_VALUE;
+  int *word = penta::status_word(ctx->device, ctx->slot);
   if (word == nullptr) return PENTAD_STATUS_INTERNAL_ERROR;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  int host = 0;
-  const int zero = 0;
-  if (cudaMemcpyAsync(&host, word, sizeof(int), cudaMemcpyDeviceToHost, s) !=
-          cudaSuccess ||
-      cudaMemcpyAsync(word, &zero, sizeof(int), cudaMemcpyHostToDevice, s) !=
-          cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess) {
+  if (penta::launch_bounded_wait_selftest(1000ull * limit_us, word,
+                                          static_cast<cudaStream_t>(stream)) != cudaSuccess) {
     cudaGetLastError();
     return PENTAD_STATUS_EXECUTION_FAILED;
   }
-  if (bits) *bits = host;
-  return (host & penta::STATUS_ZERO_PIVOT_BIT) ? PENTAD_STATUS_ZERO_PIVOT
-                                               : PENTAD_STATUS_SUCCESS;
+  return PENTAD_STATUS_SUCCESS;
 }
 
 extern "C" pentadStatus_t pentadsolver_set_algo(pentadsolver_handle_t h,
@@ -1259,6 +1336,16 @@ extern "C" const char *pentadsolver_status_string(pentadStatus_t s) {
 struct pentadsolver_plan_s {
   penta::Plan *p;
 };
+
+extern "C" pentadStatus_t pentadsolver_plan_status_check(pentadsolver_plan_t plan, void *stream,
+                                                         int *bits) {
+  if (plan == nullptr || plan->p == nullptr) return PENTAD_STATUS_INVALID_VALUE;
+  const penta::Plan &p = *plan->p;
+  const char *why = "";
+  if (!penta::on_own_device(*p.ctx, &why)) return PENTAD_STATUS_INVALID_VALUE;
+  return penta::take_status(p.ctx->device, p.report_slot(), static_cast<cudaStream_t>(stream),
+                            bits);
+}
 
 extern "C" pentadStatus_t pentadsolver_plan_buffer_size(pentadsolver_handle_t h, int elem_bytes,
                                                         int count,

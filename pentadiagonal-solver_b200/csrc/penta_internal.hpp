@@ -6,9 +6,20 @@
 #include <type_traits>
 #include <vector>
 
+#include "pentad_common.hpp"
+#include "pentadsolver_handle.hpp"
 #include "penta_lines.h"
 
 namespace penta {
+
+// penta_api.cpp: the rules every entry point applies, for entry points
+// defined elsewhere.  check_shape: the shape checks (pure host code; the
+// reference's limits, overflow-safe).  bind_handle: resolve a handle (NULL:
+// the current device's default context), bind it to the current device on
+// first use, refuse a handle bound to another device, and give the address of
+// its status word.
+pentadStatus_t check_shape(const int *dims, int ndim, int solvedim, Lines &L, const char **why);
+pentadStatus_t bind_handle(pentadsolver_handle_t h, int **status, const char **why);
 
 template <typename F> struct SolveArgs {
   const F *ds, *dl, *d, *du, *dw;
@@ -141,9 +152,20 @@ int refine_chunks(long long n_points);
 cudaError_t launch_refine_step(RefineStep step, const RefineGrid &one, const RefineGrid *table,
                                int count, int total_chunks, cudaStream_t stream);
 
-// penta_status.cu: address of the device status word of `device` (the
-// current device when the address is first taken).
-int *device_status_word(int device);
+// penta_status.cu: status words, one slot per handle or plan in a fixed
+// device array (slot 0: the handle-less calls).  Addresses are taken with
+// `device` current.
+constexpr int kStatusSlots = 4096;
+int *status_word(int device, int slot);
+int *device_status_word(int device);  // slot 0
+int status_slot_acquire();            // a free slot, or 0 when none is left
+void status_slot_release(int slot, int device);  // clears the word (synchronous)
+// *bits = atomicExch(word, 0) on `stream`, then synchronises `stream`.
+cudaError_t status_take(int device, int slot, cudaStream_t stream, int *bits);
+// A kernel whose one wait never completes: raises STATUS_TIMEOUT_BIT in
+// *status after `limit_ns`.
+cudaError_t launch_bounded_wait_selftest(unsigned long long limit_ns, int *status,
+                                         cudaStream_t stream);
 
 // Bytes of caller scratch the global-scratch kernel needs.
 template <typename F> inline size_t thomas_global_scratch(const Lines &L) {

@@ -50,13 +50,19 @@ __device__ __forceinline__ unsigned long long global_ns() {
   asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
   return t;
 }
-// Bounded wait: false when the barrier did not complete within ~2 s.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+// Bounded wait: false when the barrier did not complete within `limit_ns`.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t *bar, unsigned parity,
+                                              unsigned long long limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   while (!mbar_try_wait(bar, parity))
-    if (global_ns() - t0 > 2000000000ull) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   return true;
+}
+// The solvers' limit: ~2 s.
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+  return mbar_wait_for(bar, parity, kWaitLimitNs);
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar))

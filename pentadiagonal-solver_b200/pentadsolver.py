@@ -220,14 +220,30 @@ def gpsv_batch_legacy(ds, dl, d, du, dw, x, solvedim: int, buffer=None, handle=N
        int(solvedim), None if buffer is None else _ptr(buffer))
 
 
+#: status bits (pentadsolver_status_check)
+ZERO_PIVOT_BIT = 1
+TIMEOUT_BIT = 2
+
+
 def status_check(stream=None, handle=None) -> tuple[int, int]:
-    """Synchronise and read/clear the device status bits: (status, bits)."""
+    """Read and clear the status bits of ``handle``'s solves (the NULL
+    handle's shared word when None), then synchronise: (status, bits)."""
     sp = None
     if stream is not None:
         sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
     bits = ctypes.c_int(0)
     st = lib().pentadsolver_status_check(_hval(handle), sp, ctypes.byref(bits))
     return int(st), int(bits.value)
+
+
+def selftest_bounded_wait(limit_us: int, stream=None, handle=None) -> int:
+    """Launch the kernel whose one wait never completes; it gives up after
+    ``limit_us`` and raises TIMEOUT_BIT in the handle's status word."""
+    sp = None
+    if stream is not None:
+        sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+    return int(_typed("pentadsolver_selftest_bounded_wait", [_P, ctypes.c_uint, _P])(
+        _hval(handle), int(limit_us), sp))
 
 
 def alloc_buffer(dims, solvedim: int, dtype, device="cuda"):
@@ -369,6 +385,13 @@ class Plan:
 
     def describe(self) -> str:
         return _typed("pentadsolver_plan_describe", [_P], ctypes.c_char_p)(self._plan).decode()
+
+    def status_check(self, stream=None) -> tuple[int, int]:
+        """Read and clear this plan's own status bits, then synchronise."""
+        bits = ctypes.c_int(0)
+        st = _typed("pentadsolver_plan_status_check", [_P, _P, ctypes.POINTER(_I)])(
+            self._plan, _stream_ptr(stream, self.device), ctypes.byref(bits))
+        return int(st), int(bits.value)
 
     def estimates(self, stream=None):
         """(max|last correction|, max|x|) per grid of a refinement plan."""

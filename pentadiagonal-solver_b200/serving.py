@@ -236,6 +236,7 @@ class CudaExecutor:
         self.next_stream = 0
         self.keep_results = keep_results
         self.results = {}
+        self.status = {}   # request id -> status bits of the batch that solved it
         self.t0 = time.perf_counter()
         self.handle = ps.Handle()
 
@@ -286,13 +287,22 @@ class CudaExecutor:
             ev.record(s)
         if b.key[0] == "seq":
             ev.synchronize()   # the baseline waits for each call
-        return (ev, plan, grids)
+        return (ev, plan, grids, s)
 
     def done(self, token) -> bool:
         return token[0].query()
 
     def finish(self, b: Batch) -> None:
-        ev, plan, grids = b.handle
+        ev, plan, grids, s = b.handle
+        # the batch has finished: its status word (the plan's own, or the
+        # executor handle's for a single call) says whether any of its
+        # kernels met a zero pivot or gave up a wait
+        if hasattr(plan, "status_check"):
+            bits = plan.status_check(s)[1]
+        else:
+            bits = self.ps.status_check(s, self.handle)[1]
+        for r in b.requests:
+            self.status[r.rid] = bits
         if hasattr(plan, "close"):
             plan.close()
         if self.keep_results:

@@ -3,7 +3,9 @@
 
 Run here (it needs the reference tree, which the GPU box does not have):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref REFERENCE_TREE]
+
+(default: $PENTA_REFERENCE_DIR, else /root/reference)
 
 1. Reference fixtures.  Runs the reference's own generator
    ``test/gen_testcases.py`` (numpy seed 1, scipy ``solve_banded``) in a
@@ -128,7 +130,7 @@ def make_reference_runs() -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=str(oracle.reference_dir()))
     args = ap.parse_args()
     make_reference_fixtures(Path(args.ref))
     make_reference_runs()

@@ -24,7 +24,7 @@ import mesh
 import pentadsolver as ps
 from oracle import oracle
 
-SHIPPED = Path("/root/reference/test/cpu/singlenode/files")
+SHIPPED = oracle.reference_dir() / "test" / "cpu" / "singlenode" / "files"
 
 needs_ref = pytest.mark.skipif(not oracle.ref_mesh_available(),
                                reason="oracle/_ref/libmesh_ref.so not built")

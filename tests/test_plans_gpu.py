@@ -45,8 +45,8 @@ def test_plan_uneven_grids_match_oracle(cuda, dtype, solvedim):
     with ps.Plan(devs, solvedim) as plan:
         desc = plan.describe()
         plan.execute()
-        st, bits = ps.status_check()
-        assert bits == 0, desc
+        st, bits = plan.status_check()   # the plan's own status word
+        assert st == ps.SUCCESS and bits == 0, desc
     assert "tmem-batch" in desc, desc
     for dims, dv, ref in zip(dims_list, devs, refs):
         e = fwd_err(dv["x"].cpu().numpy(), ref)
@@ -145,6 +145,7 @@ def test_refine_plan_uneven_grids(cuda, solvedim):
         plan.execute()
         est = plan.estimates()
         desc = plan.describe()
+        assert plan.status_check() == (ps.SUCCESS, 0)
     assert "refine steps=2" in desc
     for dims, dv, ref, (dmax, xmax) in zip(dims_list, devs, refs, est):
         e = fwd_err(dv["x"].cpu().numpy(), ref)

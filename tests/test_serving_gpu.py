@@ -36,6 +36,9 @@ def test_each_result_is_the_same_alone_and_in_the_mix(cuda, policy):
         e = fwd_err(got, x.cpu().numpy())
         tol = 1e-10 if (policy == "mixed" and r.tol >= 1e-10) else 1e-12
         assert e <= tol, (r.rid, shapes[r.problem], r.solvedim, r.tol, e)
+    # every request's batch reported a clean status word of its own
+    assert sorted(ex.status) == sorted(r.rid for r in tr)
+    assert not any(ex.status.values())
     assert ps.status_check()[1] == 0
 
 

@@ -52,6 +52,40 @@ def test_noalloc_rejects_grids_beyond_its_array():
     assert 3 * 88 ** 3 * 8 <= MAX_BYTES < 3 * 89 ** 3 * 8
 
 
+@pytest.mark.parametrize("dims, solvedim", [([699051, 1, 1], 0), ([699051], 0),
+                                            ([1, 699051, 1], 1), ([3, 233017, 1], 1)])
+def test_noalloc_rejects_one_point_past_its_array(dims, solvedim):
+    # 699,051 points need 3 * 699,051 * 8 = 16,777,224 bytes: 8 past the array.
+    # Rejected by the size check itself, before any device work (pointers are
+    # placeholders that nothing dereferences).
+    assert 3 * 8 * int(np.prod(dims)) == MAX_BYTES + 8
+    st = _noalloc()(None, 1, 1, 1, 1, 1, 1, ps._dims(dims), len(dims), solvedim, None)
+    assert st == ps.INVALID_VALUE
+
+
+def test_noalloc_shape_rules_match_the_regular_entry_point():
+    # dimensions whose product overflows 64 bits, a line longer than 2^24 rows,
+    # and a non-positive extent are refused exactly as pentadsolver_buffer_size_ex
+    # refuses them, without touching the device
+    for dims, solvedim in (([1 << 30] * 8, 0), ([(1 << 24) + 1, 1, 1], 0), ([16, 0, 16], 0),
+                           ([16, 16, 16], 3), ([16] * 9, 0)):
+        st = _noalloc()(None, 1, 1, 1, 1, 1, 1, ps._dims(dims), len(dims), solvedim, None)
+        assert st == ps.INVALID_VALUE, dims
+        with pytest.raises(ps.PentadError):
+            ps.buffer_size(dims, solvedim)
+
+
+def test_noalloc_accepts_the_largest_grid_without_a_device():
+    # 699,050 points pass the size check; with no CUDA device the call then
+    # stops at binding the handle (nothing is launched)
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("only meaningful where no device can be bound")
+    st = _noalloc()(None, 1, 1, 1, 1, 1, 1, ps._dims([699050, 1, 1]), 3, 0, None)
+    assert st == ps.NOT_INITIALIZED
+
+
 @pytest.mark.gpu
 def test_noalloc_matches_regular_entry_point_on_consecutive_calls(cuda):
     import torch
