@@ -18,6 +18,12 @@ L2, so no flush is needed between steps.
 Under torchrun every rank solves its own grid (independent replicas: the
 path has no data exchange), timed with CUDA events between barriers; the
 reported time is the max over ranks and `value` counts all ranks' bytes.
+With --gpus N > 1 and no torchrun environment, the script launches N ranks
+itself (torch.distributed.run on 127.0.0.1) with the same arguments.
+
+--impl reference times the reference's own CPU solver (its AVX2 + OpenMP
+src/cpu/singlenode/pentad_cpu.cpp, compiled from its sources into
+oracle/_ref) on all host cores, each step the same 50-iteration ADI run.
 """
 from __future__ import annotations
 
@@ -157,6 +163,65 @@ def adi_problem(n: int, device, dtype):
     host["x"] = field
     dev = {k: v.to(device) for k, v in host.items()}
     return host, dev
+
+
+def spawn_ranks(n: int, argv: list[str]) -> int:
+    """Run this script as `n` ranks under torch.distributed.run (one node,
+    127.0.0.1, a free port) with the given arguments; returns the exit code
+    (rank 0 prints the JSON line)."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={n}", "--master-addr=127.0.0.1", f"--master-port={port}",
+           str(Path(__file__).resolve()), *argv]
+    return subprocess.run(cmd).returncode
+
+
+def reference_gpu_leg(d, names, n, iters=ITERS):
+    """The reference's own GPU solver (src/cuda/singlenode/pentad_cuda.cu built
+    for sm_100a, stock dispatch) on the same grid and coefficients: `iters`
+    ADI iterations timed with CUDA events on the legacy default stream it
+    launches on.  Outside every timed region of this bench."""
+    import ctypes
+
+    import torch
+
+    from oracle import oracle
+
+    if not oracle.ref_available("cuda"):
+        return {"unavailable": "oracle/_ref/libpentad_cuda_ref.so not built"}
+    solve, ran = oracle.ref_cuda_solver()
+    x = d["x"].clone()
+    buf = torch.empty(9 * n ** 3 * 8, dtype=torch.uint8, device=x.device)  # its x sizing
+    cdims = (ctypes.c_int * 3)(n, n, n)
+    ptrs = [ctypes.c_void_p(d[k].data_ptr()) for k in names] + [ctypes.c_void_p(x.data_ptr())]
+    bp = ctypes.c_void_p(buf.data_ptr())
+    legacy = torch.cuda.default_stream(x.device)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(legacy):
+        for axis in range(3):   # warm-up: module load, first launches
+            solve(None, *ptrs, cdims, 3, axis, bp)
+        torch.cuda.synchronize()
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(iters)]
+        for it in range(iters):
+            for axis in range(3):
+                ev[it][axis].record(legacy)
+                solve(None, *ptrs, cdims, 3, axis, bp)
+            ev[it][3].record(legacy)
+        torch.cuda.synchronize()
+    per_dir = [statistics.mean(ev[it][a].elapsed_time(ev[it][a + 1]) for it in range(iters))
+               for a in range(3)]
+    ms_it = ev[0][0].elapsed_time(ev[-1][3]) / iters
+    del buf
+    return {"value": round(BYTES_PER_POINT_AXIS * n ** 3 * 3 / (ms_it * 1e-3) / 1e9, 1),
+            "unit": "GB/s", "ms_per_iteration": round(ms_it, 4),
+            "per_direction_ms": [round(v, 4) for v in per_dir],
+            "kernels": [ran(a) for a in range(3)], "iterations": iters,
+            "what": "src/cuda/singlenode/pentad_cuda.cu (sm_100a, stock dispatch), same "
+                    "grid, coefficients and field; CUDA events on its launch stream"}
 
 
 def run_ours(args):
@@ -405,6 +470,13 @@ def run_ours(args):
                                   "traffic": traffic_of([slow])},
         },
     }
+    # ---- the reference's own GPU path on the same problem (not timed above) --
+    if world == 1 and not args.no_reference_gpu:
+        result["reference_gpu"] = reference_gpu_leg(d, names, n)
+        if "ms_per_iteration" in result["reference_gpu"]:
+            result["reference_gpu"]["our_speedup"] = round(
+                result["reference_gpu"]["ms_per_iteration"] / (ms_step / ITERS), 2)
+
     # ---- the same ADI run with shared factorisation (constant coefficients) --
     # Algorithmic bytes: RHS read + solution written, 2 x 8 B per point per
     # axis (the 5n-entry table is negligible).  Same field, same 50 x 3 solves.
@@ -488,15 +560,12 @@ def cpu_solver():
             "port", "oracle/penta_oracle.c")
 
 
-def cpu_baseline(n, budget_s=12.0, max_iters=1000):
-    """The reference's CPU solver on the host cores for about budget_s seconds
-    of whole ADI iterations (the bounded sample the line reports)."""
+def _cpu_sample(co, fn, threads, budget_s, max_iters=1000):
+    """Whole ADI iterations of the CPU solver with `threads` OpenMP threads for
+    about budget_s seconds: (iterations, seconds)."""
     from oracle import oracle
 
-    threads = _cpu_threads()
     oracle.set_threads(threads)
-    co = cpu_problem(n)
-    fn, kind, what = cpu_solver()
     for axis in range(3):  # warm-up (page faults, thread pool)
         fn(co, axis)
     t0 = time.perf_counter()
@@ -505,11 +574,30 @@ def cpu_baseline(n, budget_s=12.0, max_iters=1000):
         for axis in range(3):
             fn(co, axis)
         iters += 1
-    dt = time.perf_counter() - t0
+    return iters, time.perf_counter() - t0
+
+
+def cpu_baseline(n, budget_s=12.0, single_s=4.0):
+    """The reference's CPU solver on the host cores for about budget_s seconds
+    of whole ADI iterations (the bounded sample the line reports), and again
+    with one thread for about single_s seconds."""
+    from oracle import oracle
+
+    threads = _cpu_threads()
+    co = cpu_problem(n)
+    fn, kind, what = cpu_solver()
+    iters, dt = _cpu_sample(co, fn, threads, budget_s)
     gbs = BYTES_PER_POINT_AXIS * n ** 3 * 3 * iters / dt / 1e9
+    it1, dt1 = _cpu_sample(co, fn, 1, single_s)
+    gbs1 = BYTES_PER_POINT_AXIS * n ** 3 * 3 * it1 / dt1 / 1e9
+    oracle.set_threads(threads)
     return {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind,
+            "cpu_model": oracle.cpu_model(), "nproc": os.cpu_count(),
             "sample": f"{iters} ADI iterations (x,y,z) of the {n}^3 FP64 grid, {what}, "
-                      f"{dt:.1f} s"}
+                      f"{threads} threads, {dt:.1f} s",
+            "single_thread": {"value": round(gbs1, 3), "unit": "GB/s", "cores": 1,
+                              "ms_per_iteration": round(dt1 * 1e3 / max(it1, 1), 1),
+                              "sample": f"{it1} ADI iterations, 1 thread, {dt1:.1f} s"}}
 
 
 def run_reference(args):
@@ -523,16 +611,20 @@ def run_reference(args):
     n = args.n
     co = cpu_problem(n)
     fn, kind, what = cpu_solver()
+
+    def step():  # one ADI run: 50 iterations of x, y, z, as the GPU arm's step
+        for _ in range(ITERS):
+            for axis in range(3):
+                fn(co, axis)
+
     for _ in range(args.warmup):
-        for axis in range(3):
-            fn(co, axis)
+        step()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        for axis in range(3):
-            fn(co, axis)
+        step()
     dt = time.perf_counter() - t0
     ms_step = dt * 1e3 / args.steps
-    value = BYTES_PER_POINT_AXIS * n ** 3 * 3 / (ms_step * 1e-3) / 1e9
+    value = BYTES_PER_POINT_AXIS * n ** 3 * 3 * ITERS / (ms_step * 1e-3) / 1e9
     world = int(os.environ.get("WORLD_SIZE", "1"))
     print(json.dumps({
         "impl": "reference",
@@ -549,10 +641,14 @@ def run_reference(args):
         "dtype": "f64",
         "data": "synthetic (config 1 coefficients, seeded U(-1,1) field)",
         "config": {"workload": "adi_256cube_fp64_general_50iter", "grid": [n, n, n],
-                   "step": "one ADI iteration (x,y,z) of the workload, host cores",
+                   "iters_per_step": ITERS,
+                   "step": "one ADI run of 50 iterations (x,y,z), host cores",
+                   "ms_per_iteration": round(ms_step / ITERS, 3),
                    "parallelism": "host cores"},
         "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads,
-                         "kind": kind, "sample": f"{args.steps} ADI iterations, {what}"},
+                         "kind": kind, "cpu_model": oracle.cpu_model(),
+                         "nproc": os.cpu_count(),
+                         "sample": f"{args.steps} ADI runs of {ITERS} iterations, {what}"},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }))
@@ -564,12 +660,16 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--grid-edge", dest="n", type=int, default=N_DEFAULT,
+                    help="edge of the cubic grid (default 256)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus, sys.argv[1:]))
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -5,13 +5,13 @@
            axis and forward error against the CPU oracle (parity workload).
   config2  512^3 random dominant coefficients: plain FP64 against FP32 sweeps
            with 1..3 FP64 refinement steps; time, GB/s (56 B per point and
-           axis for both: the same useful work) and forward error against
-           the FP64 oracle (CPU oracle along y, the plain FP64 GPU solve --
-           itself within 1e-12 of the oracle -- along x and z).
+           axis for both: the same useful work) and forward error of every
+           result against the FP64 CPU oracle, on every axis.
   config3  96 grids, N_x, N_y, N_z ~ U[32, 384] (seeded), random dominant
            coefficients, x, y and z each one plan (one persistent launch),
            the three captured in one CUDA graph; FP64 and FP32 + 1 refinement
-           step; against per-grid single calls.
+           step (all 96 grids); against per-grid single calls.  Forward errors
+           of both forms against the CPU oracle, grid by grid.
   config4  serving: a Poisson stream (2000 requests/s) of grids with per-axis
            N ~ logU[16, 512] from a device-resident pool, solvedim U{0,1,2},
            70% at tolerance 1e-10 and 30% at 1e-13, 150 GB budget; p50/p99
@@ -37,7 +37,8 @@
            CUDA-event iteration time.
 
 All inputs are synthetic (seeded); times are CUDA-event device times except
-the serving loop and the reference's host mesh build (wall clock).  Like
+the serving loop and the reference's host mesh build (wall clock).  Every line
+carries the SM clocks and throttle reasons sampled (nvidia-smi) while it ran.  Like
 bench.py, this script uses oracle/ only as the checker (forward errors) and
 for the reference's own CPU code timed as the baseline; the solves and grids
 it measures are the library's.
@@ -113,6 +114,26 @@ def fwd_err(a, b) -> float:
     return float((a - b).abs().max() / b.abs().max())
 
 
+def oracle_errors(grids, rhs, results, axes):
+    """Largest forward error of `results` against the CPU oracle solving each
+    grid's right-hand side along `axes` in turn (grid by grid, so the host
+    holds one grid at a time)."""
+    import os
+
+    from oracle import oracle
+
+    oracle.set_threads(os.cpu_count() or 1)
+    worst = 0.0
+    for g, r, got in zip(grids, rhs, results):
+        host = {k: g[k].cpu().numpy() for k in ("ds", "dl", "d", "du", "dw")}
+        x = r.cpu().numpy()
+        for axis in axes:
+            oracle.solve(host["ds"], host["dl"], host["d"], host["du"], host["dw"], x, axis)
+        xg = got.cpu().numpy()
+        worst = max(worst, float(np.abs(xg - x).max() / np.abs(x).max()))
+    return worst
+
+
 def config0():
     import torch
 
@@ -165,16 +186,14 @@ def config2(n=512):
             copy_ms = timed(lambda: x64.copy_(b))
             plain()
             torch.cuda.synchronize()
-            ref = x64.clone()
-            err_kind = "gpu_fp64"
-            if axis == 1:  # the CPU FP64 oracle on this axis
-                host = {k: p[k].cpu().numpy() for k in ("ds", "dl", "d", "du", "dw")}
-                xr = b.cpu().numpy()
-                oracle.set_threads(__import__("os").cpu_count() or 1)
-                oracle.solve(host["ds"], host["dl"], host["d"], host["du"], host["dw"], xr, axis)
-                ref = torch.from_numpy(xr).cuda()
-                err_kind = "cpu_oracle"
-                del host
+            # the CPU FP64 oracle on this axis (the reference for every error)
+            host = {k: p[k].cpu().numpy() for k in ("ds", "dl", "d", "du", "dw")}
+            xr = b.cpu().numpy()
+            oracle.set_threads(__import__("os").cpu_count() or 1)
+            oracle.solve(host["ds"], host["dl"], host["d"], host["du"], host["dw"], xr, axis)
+            ref = torch.from_numpy(xr).cuda()
+            err_kind = "cpu_oracle"
+            del host, xr
             row = {"axis": axis, "fp64": {"ms": round(ms64 - copy_ms, 4),
                                           "variant": h.variant_that_ran(0 if axis == 0 else (2 if axis == 2 else 1)),
                                           "fwd_err": fwd_err(x64, ref)}}
@@ -245,6 +264,7 @@ def config3(n_grids=96, lo=32, hi=384, seed=33):
     graph.replay()
     torch.cuda.synchronize()
     ref = [g["x"].clone() for g in grids]
+    out["fp64_fwd_err_max_vs_oracle"] = oracle_errors(grids, rhs, ref, axes=(0, 1, 2))
     out["fp64_graph_ms_xyz"] = round(ms, 3)
     out["fp64_GBps"] = round(3 * 56 * pts / (ms * 1e-3) / 1e9, 1)
     out["fp64_systems_per_s"] = round(sum(3 * math.prod(d) / max(d) for d in dims_list) / (ms * 1e-3))
@@ -271,8 +291,8 @@ def config3(n_grids=96, lo=32, hi=384, seed=33):
     out["batched_speedup"] = round(ms_single / ms, 3)
     # FP32 sweeps + 1 refinement step: one refinement plan per axis (its FP32
     # copies of the coefficients live in its own buffer), each axis captured
-    # in a graph and timed, over the first `ir_grids` grids (device memory)
-    ir_grids = min(n_grids, 48)
+    # in a graph and timed, over all grids (x, y, z in turn, as FP64 above)
+    ir_grids = n_grids
     sub, sub_rhs, sub_ref = grids[:ir_grids], rhs[:ir_grids], ref[:ir_grids]
     pts_ir = sum(math.prod(d) for d in dims_list[:ir_grids])
     out["ir1_grids"] = ir_grids
@@ -303,7 +323,8 @@ def config3(n_grids=96, lo=32, hi=384, seed=33):
         out["ir1_ms_xyz"] = round(ms_r, 3)
         out["ir1_ms_per_axis"] = [round(v, 3) for v in ms_axes]
         out["ir1_GBps_equiv"] = round(3 * 56 * pts_ir / (ms_r * 1e-3) / 1e9, 1)
-        out["ir1_fwd_err_max_vs_fp64"] = max(fwd_err(g["x"], r) for g, r in zip(sub, sub_ref))
+        out["ir1_fwd_err_max_vs_oracle"] = oracle_errors(sub, sub_rhs,
+                                                         [g["x"] for g in sub], axes=(0, 1, 2))
     except RuntimeError as e:  # device memory
         out["ir1_error"] = str(e)[:200]
     out["peak_GBps"] = peak()
@@ -441,10 +462,14 @@ def main():
     runs = {"0": config0, "2": lambda: config2(args.n2), "3": lambda: config3(args.grids3),
             "4": lambda: config4(seconds=args.seconds4), "mesh": config_mesh,
             "refapp": config_refapp}
+    from bench import ClockSampler
+
     for c in ("0", "2", "3", "4", "mesh", "refapp"):
         if c in want:
             t0 = time.time()
-            res = runs[c]()
+            with ClockSampler(0) as clk:
+                res = runs[c]()
+            res["clocks"] = clk.summary()
             res["wall_s"] = round(time.time() - t0, 1)
             print(json.dumps(res), flush=True)
 

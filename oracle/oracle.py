@@ -174,6 +174,29 @@ def ref_solve(ds, dl, d, du, dw, x, solvedim, which: str = "orig", dims=None):
     return x
 
 
+def ref_cuda_solver():
+    """The reference's own GPU solver (``src/cuda/singlenode/pentad_cuda.cu``
+    compiled for sm_100a into ``_ref/libpentad_cuda_ref.so``), stock
+    dispatch: (D_gpsv_batch taking device pointers and a device scratch
+    buffer of its ``buffer_size_ext`` bytes, kernel_that_ran(direction))."""
+    lib = _ref_lib("cuda")
+    ran = lib.pentadsolver_kernel_that_ran
+    ran.argtypes = [ctypes.c_int]
+    ran.restype = ctypes.c_char_p
+    return lib.pentadsolver_D_gpsv_batch, (lambda direction: ran(int(direction)).decode())
+
+
+def cpu_model() -> str:
+    """The host CPU's model name (``/proc/cpuinfo``), or "unknown"."""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def set_threads(n: int) -> None:
     """OpenMP thread count for later oracle / reference calls in this process."""
     os.environ["OMP_NUM_THREADS"] = str(int(n))

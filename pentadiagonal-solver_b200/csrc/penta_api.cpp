@@ -397,12 +397,13 @@ bool pick_tmem(Context &ctx, const SolveArgs<F> &a, bool contig, size_t usable_b
                TmemConfig &out, const std::string &variant) {
   int fmode = 0;
   if (!tmem_supported<F>(a, contig, usable_buf, fmode)) return false;
+  const int loads = tmem_loads<F>(a, contig);
   int want[2] = {-1, -1};
   if (!variant.empty()) std::sscanf(variant.c_str(), "%d,%d", &want[0], &want[1]);
   const std::vector<TmemConfig> &all = tmem_configs<F>();
   for (size_t i = 0; i < all.size(); ++i) {
     const TmemConfig &c = all[i];
-    if (c.contig != contig || c.fmode != fmode) continue;
+    if (c.contig != contig || c.fmode != fmode || c.loads != loads) continue;
     if ((want[0] >= 0 && c.stages != want[0]) || (want[1] >= 0 && c.xstages != want[1]))
       continue;
     if (c.smem > (size_t)ctx.smem_optin) continue;
@@ -579,10 +580,10 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
           err = launch_tmem<F>(a, mc, ctx.sm_count, stream);
           if (err == cudaSuccess) {
             char vb[96];
-            std::snprintf(vb, sizeof vb, "thomas-pcr:tmem P2 S16 R%d x%d/%d%s%s", mc.R,
+            std::snprintf(vb, sizeof vb, "thomas-pcr:tmem P2 S16 R%d x%d/%d%s%s%s", mc.R,
                           mc.stages, mc.xstages,
                           mc.fmode == 2 ? " fbuf" : mc.fmode == 1 ? " w2s" : "",
-                          contig ? " contig" : "");
+                          mc.loads == 1 ? " bulk" : "", contig ? " contig" : "");
             record(ctx, dir, "thomas-pcr", vb);
             return PENTAD_STATUS_SUCCESS;
           }
@@ -693,6 +694,7 @@ struct Plan {
   struct Group {  // one batched launch: jobs [first, first + count) of the table
     int first, count, tiles;
     int fmode;  // factor mode of its grids
+    int loads;  // their stage layout (TMA tiles / bulk copies)
   };
   std::vector<Group> groups;
   std::vector<PlanSingle> singles;
@@ -723,14 +725,15 @@ pentadStatus_t plan_layout(Context &ctx, int count, const pentadsolver_grid_t *g
                            int solvedim, std::vector<int> &order, std::vector<size_t> &offs,
                            std::vector<PlanSingle> &singles, bool &w2s, size_t &table_bytes,
                            size_t &scratch_bytes, const char **why,
-                           std::vector<char> *grid_w2s = nullptr) {
+                           std::vector<char> *grid_w2s = nullptr,
+                           std::vector<char> *grid_loads = nullptr) {
   if (count < 1 || grids == nullptr) {
     *why = "no grids";
     return PENTAD_STATUS_INVALID_VALUE;
   }
   const bool contig = solvedim == 0;
   std::vector<Shape> shapes(count);
-  std::vector<char> ok(count, 0), need_w2s(count, 0);
+  std::vector<char> ok(count, 0), need_w2s(count, 0), loads(count, 0);
   for (int i = 0; i < count; ++i) {
     const pentadsolver_grid_t &g = grids[i];
     pentadStatus_t st = make_shape(g.dims, g.ndim, solvedim, shapes[i], why);
@@ -745,6 +748,11 @@ pentadStatus_t plan_layout(Context &ctx, int count, const pentadsolver_grid_t *g
     for (const void *p : ptrs) aligned = aligned && reinterpret_cast<uintptr_t>(p) % sizeof(F) == 0;
     ok[i] = aligned && !env_flag("PENTA_NO_TMA") && tmem_shape<F>(shapes[i].L, contig, w);
     need_w2s[i] = (char)w;
+    SolveArgs<F> ga{static_cast<const F *>(g.ds), static_cast<const F *>(g.dl),
+                    static_cast<const F *>(g.d),  static_cast<const F *>(g.du),
+                    static_cast<const F *>(g.dw), static_cast<F *>(g.x), shapes[i].L,
+                    nullptr, 0, nullptr};
+    loads[i] = (char)tmem_loads<F>(ga, contig);
   }
   (void)ctx;
   w2s = false;
@@ -755,9 +763,11 @@ pentadStatus_t plan_layout(Context &ctx, int count, const pentadsolver_grid_t *g
       w2s = w2s || need_w2s[i] != 0;
     }
   // one job group per factor mode (du2 and dw2 in TMEM; du2 alone; all in
-  // the buffer), each heaviest lines first
+  // the buffer) and stage layout (TMA tiles or bulk copies), each heaviest
+  // lines first
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
     if (need_w2s[a] != need_w2s[b]) return need_w2s[a] < need_w2s[b];
+    if (loads[a] != loads[b]) return loads[a] < loads[b];
     return shapes[a].L.n > shapes[b].L.n;
   });
   table_bytes = round256(order.size() * tmem_job_bytes<F>());
@@ -768,6 +778,7 @@ pentadStatus_t plan_layout(Context &ctx, int count, const pentadsolver_grid_t *g
     off += round256(tmem_scratch_bytes<F>(shapes[i].L, contig, need_w2s[i]));
   }
   if (grid_w2s) *grid_w2s = need_w2s;
+  if (grid_loads) *grid_loads = loads;
   singles.clear();
   for (int i = 0; i < count; ++i)
     if (!ok[i]) {
@@ -792,9 +803,9 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
   std::vector<PlanSingle> singles;
   bool w2s = false;
   size_t table_bytes = 0, scratch_bytes = 0;
-  std::vector<char> gw2s;
+  std::vector<char> gw2s, gloads;
   pentadStatus_t st = plan_layout<F>(ctx, count, grids, solvedim, order, offs, singles, w2s,
-                                     table_bytes, scratch_bytes, why, &gw2s);
+                                     table_bytes, scratch_bytes, why, &gw2s, &gloads);
   if (st != PENTAD_STATUS_SUCCESS) return st;
   if ((table_bytes > 0 && (table_buf == nullptr || table_given < table_bytes ||
                            reinterpret_cast<uintptr_t>(table_buf) % 256 != 0)) ||
@@ -828,11 +839,13 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
       *why = "host memory for the job table";
       return PENTAD_STATUS_ALLOC_FAILED;
     }
-    // fill each factor-mode group as its own tile list
+    // fill each (factor mode, stage layout) group as its own tile list
     size_t first = 0;
     while (first < order.size()) {
       size_t last = first;
-      while (last < order.size() && gw2s[order[last]] == gw2s[order[first]]) ++last;
+      while (last < order.size() && gw2s[order[last]] == gw2s[order[first]] &&
+             gloads[order[last]] == gloads[order[first]])
+        ++last;
       int tiles = 0;
       if (!tmem_fill_jobs<F>(args.data() + first, (int)(last - first), contig,
                              (int)gw2s[order[first]], base,
@@ -842,7 +855,8 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
         *why = "tensor map encoding failed";
         return PENTAD_STATUS_INTERNAL_ERROR;
       }
-      groups.push_back({(int)first, (int)(last - first), tiles, (int)gw2s[order[first]]});
+      groups.push_back({(int)first, (int)(last - first), tiles, (int)gw2s[order[first]],
+                        (int)gloads[order[first]]});
       total_tiles += tiles;
       first = last;
     }
@@ -870,9 +884,12 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
   p->ctas = (ctas > 0 && ctas < ctx.sm_count) ? ctas : ctx.sm_count;
   p->singles = singles;
   char d[160];
-  std::snprintf(d, sizeof d, "tmem-batch %s grids=%d tiles=%d launches=%d%s ctas=%d alone=%d",
+  int n_bulk = 0;
+  for (int i : order) n_bulk += gloads[i] ? 1 : 0;
+  std::snprintf(d, sizeof d,
+                "tmem-batch %s grids=%d tiles=%d launches=%d%s ctas=%d alone=%d bulk=%d",
                 sizeof(F) == 8 ? "f64" : "f32", p->n_jobs, total_tiles, (int)groups.size(),
-                w2s ? " w2s" : "", p->ctas, (int)singles.size());
+                w2s ? " w2s" : "", p->ctas, (int)singles.size(), n_bulk);
   p->desc = d;
   out = p;
   return PENTAD_STATUS_SUCCESS;
@@ -887,7 +904,7 @@ template <typename F> pentadStatus_t plan_run(Plan &p, cudaStream_t stream) {
   for (const Plan::Group &g : p.groups) {
     const cudaError_t e =
         launch_tmem_batch<F>(p.table + g.first * tmem_job_bytes<F>(), g.count, g.tiles,
-                             p.contig, g.fmode, p.discard, p.ctas, status, stream);
+                             p.contig, g.fmode, g.loads, p.discard, p.ctas, status, stream);
     if (e != cudaSuccess) {
       cudaGetLastError();
       return PENTAD_STATUS_EXECUTION_FAILED;

@@ -96,6 +96,7 @@ struct TmemConfig {
   int xstages;   // read-back stages per consumer warp
   int R;         // rows per stage
   size_t smem;   // dynamic shared memory per CTA
+  int loads;     // 0: TMA tiles / element copies; 1: bulk copies (misaligned rows or runs)
 };
 template <typename F> const std::vector<TmemConfig> &tmem_configs();
 template <typename F> int tmem_occupancy(const TmemConfig &c);
@@ -104,6 +105,8 @@ template <typename F> bool tmem_shape(const Lines &L, bool contig, int &fmode);
 template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig, int fmode);
 template <typename F>
 bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf, int &fmode);
+// The stage layout (TmemConfig::loads) a grid's loads take.
+template <typename F> int tmem_loads(const SolveArgs<F> &a, bool contig);
 template <typename F>
 cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count,
                         cudaStream_t stream);
@@ -117,7 +120,7 @@ bool tmem_fill_jobs(const SolveArgs<F> *grids, int count, bool contig, int fmode
                     int *total_tiles);
 template <typename F>
 cudaError_t launch_tmem_batch(const void *device_jobs, int n_jobs, int total_tiles, bool contig,
-                              int fmode, bool discard, int sm_count, int *status,
+                              int fmode, int loads, bool discard, int sm_count, int *status,
                               cudaStream_t stream);
 
 // shared_fact_kernels.cu: shared factorisation (line 0's coefficients for

@@ -176,6 +176,15 @@ __device__ __forceinline__ void bulk_load_hint(void *dst, const void *src, unsig
       "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
       : "memory");
 }
+// The same with the destination given as a shared-memory address.
+__device__ __forceinline__ void bulk_load_smem_hint(uint32_t dst, const void *src, unsigned bytes,
+                                                    uint64_t *bar, uint64_t pol) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1], %2, [%3], %4;\n" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+      : "memory");
+}
 __device__ __forceinline__ void st_hint(double *p, double v, uint64_t pol) {
   asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;\n" ::"l"(p), "d"(v), "l"(pol)
                : "memory");

@@ -94,6 +94,7 @@ template <typename F> struct alignas(64) TmemJob {
   F *scratch;           // this grid's region of the caller's buffer
   int n, mt, inner, tpr, n_sys, n_tiles, tile_base;
   int tma;              // 1: TMA tiles; 0: element copies (misaligned grid)
+  int bulk;             // 1: every array 16-byte aligned (bulk-copy loads possible)
 };
 
 namespace {
@@ -110,11 +111,22 @@ template <typename F, int FM> constexpr int tmem_cols_per_stage() {
   return 64 / (int)sizeof(F) * (FM == 0 ? 2 : 1) * (int)sizeof(F) / 4;
 }
 
-template <typename F, bool CONTIG, int FM, int ST, int XST> struct TmemGeom {
+// LD: how the forward stages are filled.  0: TMA tensor tiles of R x 16 (or,
+// for a misaligned grid, element copies into the same layout); 1: bulk copies
+// of 16-byte aligned supersets into a pitched layout -- each row of 16 lines
+// (strided) or each line's R rows (along x) widened by one 16-byte chunk, so a
+// grid whose rows or runs start anywhere is fetched with 16-byte requests.
+template <typename F, bool CONTIG, int FM, int ST, int XST, int LD> struct TmemGeom {
   static constexpr int R = tmem_rows_per_stage<F, CONTIG>();
+  static constexpr int EPC = 16 / (int)sizeof(F);     // elements per 16-byte chunk
   static constexpr int PW = FM == 2 ? 3 : (FM == 1 ? 2 : 1);  // scratch values per row
   static constexpr int BOX = R * TS;                  // elements per TMA tile
-  static constexpr int SE = 12 * BOX;                 // forward stage
+  // bulk layout pitches: a strided row of 16 lines + one chunk; a line's R rows
+  // + one chunk (along x)
+  static constexpr int PS = TS + EPC;
+  static constexpr int PL = R + EPC;
+  static constexpr int BOXL = LD == 0 ? BOX : (CONTIG ? TS * PL : R * PS);  // per tile
+  static constexpr int SE = 12 * BOXL;                // forward stage
   static constexpr int XE = 2 * R * TS * PW;          // read-back stage
   static constexpr int OBE = CONTIG ? 8 * BOX : 0;    // output: 2 buffers x 2 halves x 2R rows
   static constexpr int HE = 2 * 6 * 32;               // carries: 2 slots x 6 values x 32 lanes
@@ -128,6 +140,9 @@ template <typename F, bool CONTIG, int FM, int ST, int XST> struct TmemGeom {
   // at least 116 KB, so that one CTA holds an SM (and all of its TMEM)
   static constexpr size_t kSmem = kUsed > 118784 ? kUsed : 118784;
   static_assert(kSmem <= 232448, "shared memory per CTA");
+  static_assert((BOXL * sizeof(F)) % 16 == 0 && (PS * sizeof(F)) % 16 == 0 &&
+                    (PL * sizeof(F)) % 16 == 0,
+                "bulk-copy destinations must stay 16-byte aligned");
   static_assert(R * (FM == 0 ? 2 : 1) * (int)sizeof(F) / 4 == kCols, "TMEM columns per stage");
 };
 
@@ -147,13 +162,14 @@ template <> __device__ __forceinline__ float get_bits<float>(const uint32_t *tv,
   return __uint_as_float(tv[c]);
 }
 
-template <typename F, bool CONTIG, int FM, int ST, int XST, bool BATCH>
+template <typename F, bool CONTIG, int FM, int ST, int XST, int LD, bool BATCH>
 __global__ void __launch_bounds__(96 * NCONS, 1)
 tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__restrict__ jobs,
                    int n_jobs, int total_tiles, int flags, int *__restrict__ status_word) {
-  using G = TmemGeom<F, CONTIG, FM, ST, XST>;
+  using G = TmemGeom<F, CONTIG, FM, ST, XST, LD>;
   using V2 = typename Vec2<F>::T;
   constexpr int R = G::R, BOX = G::BOX, SE = G::SE, XE = G::XE, PW = G::PW, NB = G::NB;
+  constexpr int BOXL = G::BOXL, PS = G::PS, PL = G::PL;
   constexpr int EPC = 16 / (int)sizeof(F);  // elements per 16-byte chunk
   constexpr int CW = (int)sizeof(F) / 4;    // TMEM columns per value
   constexpr int kMirror[6] = {4, 3, 2, 1, 0, 5};
@@ -260,11 +276,11 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
       const TmemJob<F> *J = job_of(t, cursor);
       if (J != JG.J || ti == 0) {
         load_geo(J, JG);
-        if (!JG.tma)
+        if (LD == 1 || !JG.tma)
 #pragma unroll
           for (int q = 0; q < 6; ++q) arrs[q] = J->arr[q];
       }
-      const bool tma = JG.tma != 0;
+      const bool tma = LD == 0 && JG.tma != 0;
       if (BATCH && cursor != fenced) {  // a new grid: its maps, and the next grid's
         if (lane == 0) {
           if (tma)
@@ -296,7 +312,71 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         const int r_up = g * R;
         const int r_dn = 2 * mt - (g + 1) * R;  // lower half, virtual rows included
         F *dst = ring + slot * SE;
-        if (tma) {
+        if constexpr (LD == 1) {
+          // Bulk copies of 16-byte aligned supersets.  Copy k of the stage:
+          // tile bx = 2 q + half, then line (along x) or row (strided) `sub`.
+          // Each lane arrives once with its own byte count, then issues its
+          // copies; rows past n, lines past the grid and tiles past the run are
+          // not fetched.  A window whose last 16-byte chunk would reach past
+          // the array's end takes those few elements with plain loads (before
+          // the arrival that publishes them), so nothing outside the arrays
+          // is read.
+          constexpr int NCP = CONTIG ? 12 * TS : 12 * R;  // copies per stage
+          constexpr int KC = NCP / 32;
+          static_assert(NCP % 32 == 0, "copies per lane");
+          const long long npts = (long long)n * JG.n_sys;  // elements per array
+          const F *srcs[KC];
+          uint32_t dsts[KC];
+          unsigned nbs[KC];
+          unsigned mine = 0;
+#pragma unroll
+          for (int kk = 0; kk < KC; ++kk) {
+            const int k = lane + 32 * kk;
+            const int bx = CONTIG ? k / TS : k / R;
+            const int sub = CONTIG ? k % TS : k % R;
+            const int q = bx >> 1, h = bx & 1;
+            // the array (mirrored for the lower half: ds<->dw, dl<->du), picked
+            // by selects so that `arrs` stays in registers
+            const int aq = h ? (q < 5 ? 4 - q : 5) : q;
+            const F *src = arrs[0];
+#pragma unroll
+            for (int j = 1; j < 6; ++j)
+              if (aq == j) src = arrs[j];
+            long long off;
+            int cnt;
+            if (CONTIG) {
+              const int line = c0 + sub;
+              const int row0 = h ? r_dn : r_up;
+              cnt = (line < JG.n_sys && row0 < n) ? min(R, n - row0) : 0;
+              off = (long long)line * n + row0;
+            } else {
+              const int row = (h ? r_dn : r_up) + sub;
+              cnt = row < n ? min(TS, inner - c0) : 0;
+              off = (long long)c2 * inner * n + (long long)row * inner + c0;
+            }
+            F *const tdst = dst + bx * BOXL + sub * (CONTIG ? PL : PS);
+            nbs[kk] = 0;
+            if (cnt > 0) {
+              const long long first = off & ~(long long)(EPC - 1);
+              const long long last = off + cnt;  // exclusive, <= npts
+              long long end = (last + EPC - 1) & ~(long long)(EPC - 1);
+              if (end > npts) {
+                end = npts & ~(long long)(EPC - 1);
+                for (long long e = end > off ? end : off; e < last; ++e) tdst[e - first] = src[e];
+              }
+              if (end > first) {
+                nbs[kk] = (unsigned)((end - first) * (long long)sizeof(F));
+                srcs[kk] = src + first;
+                dsts[kk] = smem_u32(tdst);
+                mine += nbs[kk];
+              }
+            }
+          }
+          mbar_expect_tx(&full[slot], mine);
+#pragma unroll
+          for (int kk = 0; kk < KC; ++kk)
+            if (nbs[kk] != 0) bulk_load_smem_hint(dsts[kk], srcs[kk], nbs[kk], &full[slot], pol_in);
+        } else if (tma) {
           if (lane == 0) {
             const bool lower = r_dn < n;  // else all rows are virtual: not loaded
             mbar_arrive_n(&full[slot], 31);  // for the lanes that copy nothing
@@ -418,6 +498,28 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
                      (FM == 2 ? part * mt * TS * PW + sys : (part * mt * TS + sys) * PW);
       const bool flip = (ti & 1) != 0;
       const int free_blocks = NB - n_prev;  // blocks the previous tile never used
+      // bulk layout: where this lane's r-th row of a stage sits in its half's
+      // tile.  The window of a line (x) or a row (strided) starts at the
+      // 16-byte chunk holding its first element; the element's offset in that
+      // chunk is the shift.  Stages start at multiples of R rows (R a multiple
+      // of the chunk), so a tile's shifts repeat from stage to stage.
+      int ldm[LD == 1 ? R : 1];
+      if constexpr (LD == 1) {
+        if constexpr (CONTIG) {
+          const int sh = (int)(((long long)(c0 + sys) * n) & (G::EPC - 1));
+#pragma unroll
+          for (int r = 0; r < R; ++r)
+            ldm[r] = part * BOXL + sys * PL + sh + (part ? (R - 1 - r) : r);
+        } else {
+          const int s0 = (int)(((long long)c2 * JG.inner * n) & (G::EPC - 1));
+          const int im = JG.inner & (G::EPC - 1);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int rr = part ? (R - 1 - r) : r;
+            ldm[r] = part * BOXL + rr * PS + ((s0 + rr * im) & (G::EPC - 1)) + sys;
+          }
+        }
+      }
       Carry<F> c;
       c.zero();
       for (int g = 0; g < n_stages; ++g) {
@@ -427,7 +529,12 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         }
         const F *v = ring + slot * SE;
         F a[R][6];
-        if constexpr (CONTIG) {
+        if constexpr (LD == 1) {
+#pragma unroll
+          for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int q = 0; q < 6; ++q) a[r][q] = v[ldm[r] + q * 2 * BOXL];
+        } else if constexpr (CONTIG) {
           // the lower half runs its tile backwards: the pair's odd row first
 #pragma unroll
           for (int q = 0; q < 6; ++q)
@@ -881,6 +988,15 @@ bool shape_ok(const Lines &L, bool contig, int &fmode) {
   return true;
 }
 
+// Bulk-copy loads apply when every array starts on a 16-byte boundary (any
+// row stride).
+template <typename F> bool bulk_ok(const SolveArgs<F> &a) {
+  const void *ptrs[6] = {a.ds, a.dl, a.d, a.du, a.dw, a.x};
+  for (const void *p : ptrs)
+    if (reinterpret_cast<uintptr_t>(p) % 16 != 0) return false;
+  return true;
+}
+
 // TMA applies when the row stride and every array are 16-byte aligned.
 template <typename F> bool tma_ok(const SolveArgs<F> &a, bool contig) {
   if (tensor_map_encoder() == nullptr) return false;
@@ -902,6 +1018,7 @@ bool fill_job(TmemJob<F> &J, const SolveArgs<F> &a, bool contig, F *scratch, int
   const int R = contig ? tmem_rows_per_stage<F, true>() : tmem_rows_per_stage<F, false>();
   const F *ptrs[6] = {a.ds, a.dl, a.d, a.du, a.dw, a.x};
   J.tma = tma_ok<F>(a, contig) ? 1 : 0;
+  J.bulk = bulk_ok<F>(a) ? 1 : 0;
   for (int q = 0; q < 6; ++q) {
     J.arr[q] = ptrs[q];
     if (J.tma && !encode<F>(&J.maps[q], ptrs[q], a.L, contig, R)) J.tma = 0;
@@ -919,12 +1036,12 @@ bool fill_job(TmemJob<F> &J, const SolveArgs<F> &a, bool contig, F *scratch, int
   return true;
 }
 
-template <typename F, bool CONTIG, int FM, int ST, int XST, bool BATCH>
+template <typename F, bool CONTIG, int FM, int ST, int XST, int LD, bool BATCH>
 cudaError_t tmem_launch_raw(const TmemJob<F> &job1, const TmemJob<F> *jobs, int n_jobs,
                             int total_tiles, int flags, int sm_count, int *status,
                             cudaStream_t stream) {
-  using G = TmemGeom<F, CONTIG, FM, ST, XST>;
-  auto kern = tmem_thomas_kernel<F, CONTIG, FM, ST, XST, BATCH>;
+  using G = TmemGeom<F, CONTIG, FM, ST, XST, LD>;
+  auto kern = tmem_thomas_kernel<F, CONTIG, FM, ST, XST, LD, BATCH>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)G::kSmem);
   if (err != cudaSuccess) return err;
@@ -949,9 +1066,9 @@ cudaError_t tmem_launch_raw(const TmemJob<F> &job1, const TmemJob<F> *jobs, int 
   return cudaGetLastError();
 }
 
-template <typename F, bool CONTIG, int FM, int ST, int XST> int tmem_occ() {
-  using G = TmemGeom<F, CONTIG, FM, ST, XST>;
-  auto kern = tmem_thomas_kernel<F, CONTIG, FM, ST, XST, false>;
+template <typename F, bool CONTIG, int FM, int ST, int XST, int LD> int tmem_occ() {
+  using G = TmemGeom<F, CONTIG, FM, ST, XST, LD>;
+  auto kern = tmem_thomas_kernel<F, CONTIG, FM, ST, XST, LD, false>;
   int blocks = 0;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)G::kSmem) != cudaSuccess ||
@@ -965,41 +1082,54 @@ template <typename F, bool CONTIG, int FM, int ST, int XST> int tmem_occ() {
 
 }  // namespace
 
-// (type, contiguous, dw2 in the buffer, forward stages, read-back stages); for
-// each (type, layout, mode) the first variant is the default.  Batched
-// launches use the default variants.  Along x in FP64 two forward stages beat
-// three: fewer 64-byte requests in flight per line keep HBM row hits up
-// (measured at 256^3 and 512^3); FP32 along x, with 16 rows a stage, and the
-// strided directions want three.
-#define PENTA_TMEM_CONFIGS(X) \
-  X(double, true, 0, 2, 4)    \
-  X(double, true, 0, 3, 4)    \
-  X(double, true, 0, 3, 3)    \
-  X(double, false, 0, 3, 4)   \
-  X(double, false, 0, 3, 3)   \
-  X(double, false, 0, 2, 4)   \
-  X(double, true, 1, 2, 3)    \
-  X(double, true, 1, 3, 2)    \
-  X(double, false, 1, 3, 4)   \
-  X(double, true, 2, 2, 2)    \
-  X(double, false, 2, 3, 2)   \
-  X(float, true, 0, 3, 4)     \
-  X(float, true, 0, 2, 4)     \
-  X(float, false, 0, 3, 4)    \
-  X(float, false, 0, 4, 3)    \
-  X(float, true, 1, 2, 3)     \
-  X(float, true, 1, 3, 2)     \
-  X(float, false, 1, 3, 4)    \
-  X(float, true, 2, 2, 2)     \
-  X(float, false, 2, 3, 2)
+// (type, contiguous, factor mode, forward stages, read-back stages, loads);
+// for each (type, layout, mode, loads) the first variant is the default.
+// Batched launches use the default variants.  Along x in FP64 two forward
+// stages beat three: fewer 64-byte requests in flight per line keep HBM row
+// hits up (measured at 256^3 and 512^3); FP32 along x, with 16 rows a stage,
+// and the strided directions want three.  The bulk-load variants (loads = 1)
+// have wider stages, so some take fewer of them to fit shared memory.
+#define PENTA_TMEM_CONFIGS(X)   \
+  X(double, true, 0, 2, 4, 0)   \
+  X(double, true, 0, 3, 4, 0)   \
+  X(double, true, 0, 3, 3, 0)   \
+  X(double, false, 0, 3, 4, 0)  \
+  X(double, false, 0, 3, 3, 0)  \
+  X(double, false, 0, 2, 4, 0)  \
+  X(double, true, 1, 2, 3, 0)   \
+  X(double, true, 1, 3, 2, 0)   \
+  X(double, false, 1, 3, 4, 0)  \
+  X(double, true, 2, 2, 2, 0)   \
+  X(double, false, 2, 3, 2, 0)  \
+  X(float, true, 0, 3, 4, 0)    \
+  X(float, true, 0, 2, 4, 0)    \
+  X(float, false, 0, 3, 4, 0)   \
+  X(float, false, 0, 4, 3, 0)   \
+  X(float, true, 1, 2, 3, 0)    \
+  X(float, true, 1, 3, 2, 0)    \
+  X(float, false, 1, 3, 4, 0)   \
+  X(float, true, 2, 2, 2, 0)    \
+  X(float, false, 2, 3, 2, 0)   \
+  X(double, true, 0, 2, 4, 1)   \
+  X(double, false, 0, 3, 4, 1)  \
+  X(double, true, 1, 2, 3, 1)   \
+  X(double, false, 1, 2, 4, 1)  \
+  X(double, true, 2, 2, 2, 1)   \
+  X(double, false, 2, 2, 2, 1)  \
+  X(float, true, 0, 2, 4, 1)    \
+  X(float, false, 0, 3, 4, 1)   \
+  X(float, true, 1, 2, 3, 1)    \
+  X(float, false, 1, 2, 4, 1)   \
+  X(float, true, 2, 2, 2, 1)    \
+  X(float, false, 2, 2, 2, 1)
 
 template <typename F> const std::vector<TmemConfig> &tmem_configs() {
   static const std::vector<TmemConfig> v = [] {
     std::vector<TmemConfig> out;
-#define PENTA_X(FT_, C_, W_, ST_, XST_)                                                  \
+#define PENTA_X(FT_, C_, W_, ST_, XST_, LD_)                                             \
   if (std::is_same<F, FT_>::value)                                                       \
-    out.push_back(TmemConfig{C_, W_, ST_, XST_, TmemGeom<FT_, C_, W_, ST_, XST_>::R,     \
-                             TmemGeom<FT_, C_, W_, ST_, XST_>::kSmem});
+    out.push_back(TmemConfig{C_, W_, ST_, XST_, TmemGeom<FT_, C_, W_, ST_, XST_, LD_>::R, \
+                             TmemGeom<FT_, C_, W_, ST_, XST_, LD_>::kSmem, LD_});
     PENTA_TMEM_CONFIGS(PENTA_X)
 #undef PENTA_X
     return out;
@@ -1008,10 +1138,10 @@ template <typename F> const std::vector<TmemConfig> &tmem_configs() {
 }
 
 template <typename F> int tmem_occupancy(const TmemConfig &c) {
-#define PENTA_X(FT_, C_, W_, ST_, XST_)                                                  \
+#define PENTA_X(FT_, C_, W_, ST_, XST_, LD_)                                             \
   if (std::is_same<F, FT_>::value && c.contig == C_ && c.fmode == W_ && c.stages == ST_ && \
-      c.xstages == XST_)                                                                 \
-    return tmem_occ<FT_, C_, W_, ST_, XST_>();
+      c.xstages == XST_ && c.loads == LD_)                                               \
+    return tmem_occ<FT_, C_, W_, ST_, XST_, LD_>();
   PENTA_TMEM_CONFIGS(PENTA_X)
 #undef PENTA_X
   return 0;
@@ -1023,6 +1153,20 @@ template <typename F> bool tmem_shape(const Lines &L, bool contig, int &fmode) {
 
 template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig, int fmode) {
   return job_scratch_bytes<F>(L, contig, fmode);
+}
+
+// Which stage layout a grid's loads use: 0 for TMA tiles (aligned grids) or
+// element copies (arrays not 16-byte aligned), 1 for bulk copies (arrays
+// 16-byte aligned, rows or runs not).  PENTA_TMEM_LOADS=bulk also sends
+// aligned grids through bulk copies, =element keeps misaligned grids on
+// element copies (both for measurements and tests).
+template <typename F> int tmem_loads(const SolveArgs<F> &a, bool contig) {
+  const char *e = std::getenv("PENTA_TMEM_LOADS");
+  const bool force_bulk = e != nullptr && !std::strcmp(e, "bulk");
+  const bool no_bulk = e != nullptr && !std::strcmp(e, "element");
+  if (no_bulk || !bulk_ok<F>(a)) return 0;
+  if (force_bulk) return 1;
+  return tma_ok<F>(a, contig) ? 0 : 1;
 }
 
 template <typename F>
@@ -1066,16 +1210,17 @@ cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count
   TmemJob<F> J;
   if (!fill_job<F>(J, a, c.contig, static_cast<F *>(a.scratch), 0))
     return cudaErrorInvalidValue;
+  if (c.loads == 1 && !J.bulk) return cudaErrorInvalidValue;  // bulk loads need aligned arrays
   int flags = ((reinterpret_cast<uintptr_t>(a.scratch) % 128 == 0) ? 1 : 0);
   const int capped = scratch_grid_cap<F>(a, c, J.n_tiles, sm_count);
   // streamed loads evict-first when the grid is capped, and for FP32 along x with
   // dw2 in the buffer (1024 x 128 x 128: 118 against 129 us with normal priority)
   if (capped < sm_count || (sizeof(F) == 4 && c.contig && c.fmode == 1)) flags |= 2;
   sm_count = capped;
-#define PENTA_X(FT_, C_, W_, ST_, XST_)                                                   \
+#define PENTA_X(FT_, C_, W_, ST_, XST_, LD_)                                              \
   if (std::is_same<F, FT_>::value && c.contig == C_ && c.fmode == W_ && c.stages == ST_ &&  \
-      c.xstages == XST_)                                                                  \
-    return tmem_launch_raw<FT_, C_, W_, ST_, XST_, false>(                                \
+      c.xstages == XST_ && c.loads == LD_)                                                \
+    return tmem_launch_raw<FT_, C_, W_, ST_, XST_, LD_, false>(                           \
         reinterpret_cast<const TmemJob<FT_> &>(J), nullptr, 1, J.n_tiles, flags, sm_count, \
         a.status, stream);
   PENTA_TMEM_CONFIGS(PENTA_X)
@@ -1104,7 +1249,7 @@ bool tmem_fill_jobs(const SolveArgs<F> *grids, int count, bool contig, int fmode
 
 template <typename F>
 cudaError_t launch_tmem_batch(const void *device_jobs, int n_jobs, int total_tiles, bool contig,
-                              int fmode, bool discard, int sm_count, int *status,
+                              int fmode, int loads, bool discard, int sm_count, int *status,
                               cudaStream_t stream) {
   TmemJob<F> none;
   std::memset(&none, 0, sizeof(none));
@@ -1112,30 +1257,21 @@ cudaError_t launch_tmem_batch(const void *device_jobs, int n_jobs, int total_til
   // the load policy of single-grid launches (launch_tmem) on an uncapped grid:
   // evict-first streamed loads for FP32 along x with dw2 in the buffer
   const int flags = (discard ? 1 : 0) | ((sizeof(F) == 4 && contig && fmode == 1) ? 2 : 0);
-  if (contig && fmode == 0) {
-    // three forward stages along x in FP32 (85.5 against 86.4 us at 256^3), two in FP64
-    // (162 against 173 us)
-    if constexpr (sizeof(F) == 4)
-      return tmem_launch_raw<F, true, 0, 3, 4, true>(none, jobs, n_jobs, total_tiles, flags,
-                                                     sm_count, status, stream);
-    else
-      return tmem_launch_raw<F, true, 0, 2, 4, true>(none, jobs, n_jobs, total_tiles, flags,
-                                                     sm_count, status, stream);
+  // the default variant of each (layout, factor mode, loads)
+  const std::vector<TmemConfig> &all = tmem_configs<F>();
+  for (const TmemConfig &c : all) {
+    if (c.contig != contig || c.fmode != fmode || c.loads != loads) continue;
+#define PENTA_X(FT_, C_, W_, ST_, XST_, LD_)                                              \
+  if (std::is_same<F, FT_>::value && c.contig == C_ && c.fmode == W_ && c.stages == ST_ &&  \
+      c.xstages == XST_ && c.loads == LD_)                                                \
+    return tmem_launch_raw<FT_, C_, W_, ST_, XST_, LD_, true>(                            \
+        reinterpret_cast<const TmemJob<FT_> &>(none),                                     \
+        reinterpret_cast<const TmemJob<FT_> *>(jobs), n_jobs, total_tiles, flags, sm_count, \
+        status, stream);
+    PENTA_TMEM_CONFIGS(PENTA_X)
+#undef PENTA_X
   }
-  if (contig && fmode == 1)
-    return tmem_launch_raw<F, true, 1, 2, 3, true>(none, jobs, n_jobs, total_tiles, flags,
-                                                   sm_count, status, stream);
-  if (contig)
-    return tmem_launch_raw<F, true, 2, 2, 2, true>(none, jobs, n_jobs, total_tiles, flags,
-                                                   sm_count, status, stream);
-  if (fmode == 0)
-    return tmem_launch_raw<F, false, 0, 3, 4, true>(none, jobs, n_jobs, total_tiles, flags,
-                                                    sm_count, status, stream);
-  if (fmode == 1)
-    return tmem_launch_raw<F, false, 1, 3, 4, true>(none, jobs, n_jobs, total_tiles, flags,
-                                                    sm_count, status, stream);
-  return tmem_launch_raw<F, false, 2, 3, 2, true>(none, jobs, n_jobs, total_tiles, flags,
-                                                  sm_count, status, stream);
+  return cudaErrorInvalidConfiguration;
 }
 
 template const std::vector<TmemConfig> &tmem_configs<double>();
@@ -1158,9 +1294,11 @@ template bool tmem_fill_jobs<double>(const SolveArgs<double> *, int, bool, int, 
                                      void *, size_t *, int *);
 template bool tmem_fill_jobs<float>(const SolveArgs<float> *, int, bool, int, unsigned char *,
                                     void *, size_t *, int *);
-template cudaError_t launch_tmem_batch<double>(const void *, int, int, bool, int, bool, int,
-                                               int *, cudaStream_t);
-template cudaError_t launch_tmem_batch<float>(const void *, int, int, bool, int, bool, int,
+template cudaError_t launch_tmem_batch<double>(const void *, int, int, bool, int, int, bool,
+                                               int, int *, cudaStream_t);
+template cudaError_t launch_tmem_batch<float>(const void *, int, int, bool, int, int, bool, int,
                                               int *, cudaStream_t);
+template int tmem_loads<double>(const SolveArgs<double> &, bool);
+template int tmem_loads<float>(const SolveArgs<float> &, bool);
 
 }  // namespace penta

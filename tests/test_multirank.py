@@ -70,7 +70,7 @@ def test_reference_arm_prints_on_rank_zero_only():
 
 def test_reference_arm_line_carries_the_contract_keys():
     p = subprocess.run([sys.executable, str(REPO / "bench.py"), "--impl", "reference",
-                        "--steps", "3", "--warmup", "3", "--n", "64"],
+                        "--steps", "3", "--warmup", "3", "--grid-edge", "64"],
                        capture_output=True, text=True, timeout=300)
     assert p.returncode == 0, p.stderr
     line = json.loads(p.stdout.strip().splitlines()[-1])
@@ -90,3 +90,20 @@ def test_reference_arm_line_carries_the_contract_keys():
     assert line["e2e"] == {"value": line["value"], "unit": "GB/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
     assert line["config"]["workload"] == "adi_256cube_fp64_general_50iter"
+
+
+def test_gpus_n_without_torchrun_spawns_n_ranks():
+    # `bench.py --gpus 2` outside torchrun launches two ranks itself
+    # (torch.distributed.run on 127.0.0.1); the reference arm then runs on
+    # rank 0 alone, which prints the one JSON line, and rank 1 exits cleanly
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT")}
+    p = subprocess.run([sys.executable, str(REPO / "bench.py"), "--impl", "reference",
+                        "--gpus", "2", "--steps", "1", "--warmup", "3", "--grid-edge", "32"],
+                       env=env, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, p.stdout
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["n_gpus"] == 2
+    assert line["config"]["iters_per_step"] == 50 and line["value"] > 0

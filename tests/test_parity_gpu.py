@@ -380,3 +380,64 @@ def test_long_lines_factors_in_the_buffer(cuda, dims, solvedim, dtype):
     long_line = n > (512 if eb == 8 else 1024)
     if _tmem_ok(dims, solvedim, eb):
         assert "tmem" in var and (("fbuf" in var) == long_line), (dims, var)
+
+
+# Odd extents along every axis, partial tiles of 16 lines, and element counts
+# whose last 16-byte chunk is partial (the bulk windows at the array's end take
+# their last elements with plain loads).
+MISALIGNED_DIMS = [(33, 17, 9), (255, 7, 5), (17, 255, 3), (9, 7, 255), (50, 13, 7),
+                   (31, 31, 31), (66, 34, 18), (129, 3, 65)]
+
+
+def _loads_run(co, solvedim, loads, monkeypatch):
+    monkeypatch.setenv("PENTA_TMEM_LOADS", loads)
+    dv = to_dev(co)
+    dirn = direction(3, solvedim)
+    with ps.Handle() as h:
+        solve_dev(dv, solvedim, handle=h)
+        var = h.variant_that_ran(dirn)
+    monkeypatch.delenv("PENTA_TMEM_LOADS")
+    return dv["x"].cpu().numpy(), var
+
+
+@pytest.mark.parametrize("dims", MISALIGNED_DIMS)
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_misaligned_grids_bulk_element_and_tma_loads_agree(cuda, dims, dtype, monkeypatch):
+    """Rows (x) or runs (y, z) that do not start on 16-byte boundaries: the
+    Tensor-Memory kernel fetches them by bulk copies of aligned supersets
+    (default), or by element copies (PENTA_TMEM_LOADS=element); aligned
+    rows and runs by TMA tiles, or by bulk copies when forced.  The same
+    arithmetic runs on the same values whichever way they arrive, so the
+    results are identical bit for bit, and equal the oracle's."""
+    eb = np.dtype(dtype).itemsize
+    co = fixtures.random_dominant(dims, 91, dtype)
+    for solvedim in range(3):
+        n = dims[solvedim]
+        inner = int(np.prod(dims[:solvedim]))
+        if n <= 4 or not _tmem_ok(dims, solvedim, eb):
+            continue
+        aligned = ((n if solvedim == 0 else inner) * eb) % 16 == 0
+        ref = co["x"].copy()
+        oracle.solve(co["ds"], co["dl"], co["d"], co["du"], co["dw"], ref, solvedim)
+        x_auto, v_auto = _loads_run(co, solvedim, "", monkeypatch)
+        x_elem, v_elem = _loads_run(co, solvedim, "element", monkeypatch)
+        x_bulk, v_bulk = _loads_run(co, solvedim, "bulk", monkeypatch)
+        assert "tmem" in v_auto and "tmem" in v_elem and "tmem" in v_bulk
+        assert ("bulk" in v_auto) == (not aligned), (dims, solvedim, v_auto)
+        assert "bulk" not in v_elem and "bulk" in v_bulk, (v_elem, v_bulk)
+        assert fwd_err(x_auto, ref) <= FWD_TOL[dtype], (dims, solvedim, v_auto)
+        assert np.array_equal(x_auto.view(np.uint8), x_elem.view(np.uint8)), (dims, solvedim)
+        assert np.array_equal(x_auto.view(np.uint8), x_bulk.view(np.uint8)), (dims, solvedim)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_bulk_loads_on_aligned_grids_equal_tma_tiles(cuda, dtype, monkeypatch):
+    for dims in ((64, 48, 40), (256, 16, 8), (16, 20, 512)):
+        co = fixtures.random_dominant(dims, 17, dtype)
+        for solvedim in range(3):
+            if not _tmem_ok(dims, solvedim, np.dtype(dtype).itemsize):
+                continue
+            x_tma, v_tma = _loads_run(co, solvedim, "", monkeypatch)
+            x_bulk, v_bulk = _loads_run(co, solvedim, "bulk", monkeypatch)
+            assert "tmem" in v_tma and "bulk" not in v_tma and "bulk" in v_bulk, (v_tma, v_bulk)
+            assert np.array_equal(x_tma.view(np.uint8), x_bulk.view(np.uint8)), (dims, solvedim)
