@@ -248,6 +248,13 @@ def config3(n_grids=96, lo=32, hi=384, seed=33):
             g["x"].copy_(r)
 
     restore_ms = timed(restore)
+    # the library's autotuner picks each plan's CTA count (recorded in its
+    # tuning table, which plan creation with ctas = 0 then consults)
+    import autotune
+
+    tuner = autotune.Autotuner(reps=3)
+    out["tuned_ctas_fp64"] = [tuner.tune_plan(grids, axis)["best"]["ctas"] for axis in range(3)]
+    torch.cuda.empty_cache()
     # FP64 plans, captured together; the three share one scratch region
     shared = ps.aligned_bytes(max(ps.plan_sizes(grids, a)[1] for a in range(3)))
     plans = [ps.Plan(grids, axis, scratch=shared) for axis in range(3)]
@@ -300,7 +307,10 @@ def config3(n_grids=96, lo=32, hi=384, seed=33):
         for g, r in zip(sub, sub_rhs):
             g["x"].copy_(r)
         ms_axes = []
+        out["tuned_ctas_ir1"] = []
         for axis in range(3):
+            out["tuned_ctas_ir1"].append(tuner.tune_plan(sub, axis, refine_steps=1)["best"]["ctas"])
+            torch.cuda.empty_cache()
             rp = ps.Plan(sub, axis, refine_steps=1)
             saved = [g["x"].clone() for g in sub]
 

@@ -126,6 +126,13 @@ EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_create_split(
 EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_execute(pentadsolver_plan_t plan,
                                                               void *stream);
 EXTERN_C PENTAD_API const char *pentadsolver_plan_describe(pentadsolver_plan_t plan);
+/* Times `reps` executes of the plan with each of several CTA counts (all SMs,
+ * 90%, 75%, 50%), keeps the fastest for this plan and records it in the
+ * tuning table for plans of its class (see pentadsolver_tuning_key).  The
+ * executes solve the grids in place again and again.  Synchronises `stream`. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_autotune_plan(pentadsolver_plan_t plan,
+                                                              int reps, void *stream,
+                                                              int *best_ctas);
 /* As pentadsolver_status_check, for the kernels of this plan's executes: every
  * plan reports into a status word of its own. */
 EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_status_check(pentadsolver_plan_t plan,
@@ -162,6 +169,53 @@ EXTERN_C PENTAD_API pentadStatus_t pentadsolver_refine_plan_create(
     int steps, void *buffer, size_t buffer_bytes, int ctas, pentadsolver_plan_t *plan);
 EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_estimates(pentadsolver_plan_t plan,
                                                                void *stream, double *out);
+
+/* ---- Autotuning ----------------------------------------------------------
+ * No counterpart in the reference (whose selection is the fixed heuristic of
+ * src/cuda/singlenode/pentad_cuda.cu:1143-1174 plus PENTA_PCR_LANES).  A
+ * process-wide tuning table maps a shape class to the kernel choice that
+ * measured fastest; the class key is
+ *     <GPU name>|<solve, plan or refine>|<f64 or f32>|<x or yz>|n<N>|l<L>
+ * with N the line length (a plan: its longest) and L the number of lines (a
+ * plan: all of them), each rounded up to a power of two.  The automatic
+ * selection of every handle consults it for shapes that neither environment
+ * selectors nor the handle's own choices fix, and plan creation with ctas = 0
+ * takes its CTA count from it -- so a caller of the reference's interface
+ * gets tuned kernels without code changes.  On first use the table is read
+ * from the file named by PENTA_TUNING_CACHE when that variable is set; files
+ * hold one entry per line, "key<TAB>spec<TAB>algo<TAB>lanes<TAB>ctas<TAB>ms"
+ * (spec as pentadsolver_set_tuning takes it, "auto" for none). */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_tuning_load(const char *path);
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_tuning_save(const char *path);
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_tuning_clear(void);
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_tuning_set(const char *key, const char *spec,
+                                                           const char *algo, int lanes,
+                                                           int ctas, double ms);
+/* The entry for `key` as "spec<TAB>algo<TAB>lanes<TAB>ctas<TAB>ms";
+ * PENTAD_STATUS_INVALID_VALUE when there is none or `len` is too small. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_tuning_lookup(const char *key, char *out,
+                                                              size_t len);
+/* The key of a shape (`kind` "solve", "plan" or "refine"; for plans the
+ * grid's own line length and lines); `gpu_name` NULL: the current device. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_tuning_key(const char *gpu_name,
+                                                           const char *kind, int elem_bytes,
+                                                           const int *t_dims, int t_ndim,
+                                                           int t_solvedim, char *out,
+                                                           size_t len);
+/* Times, on the caller's problem and stream, each candidate kernel choice --
+ * the Tensor-Memory kernel's ring variants, the older TMA kernels, the
+ * cp.async kernel with two lanes or one lane per line -- `reps` solves each,
+ * records the fastest in the tuning table for this shape's class, and writes
+ * a report (one line per distinct kernel variant, fastest first:
+ * "label<TAB>spec<TAB>algo<TAB>lanes<TAB>variant<TAB>ms") when `report` is
+ * not NULL.  The trial solves overwrite x; `x_save` (device memory of x's
+ * size, or NULL) keeps it and puts it back at the end.  Synchronises
+ * `stream`. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_autotune_solve(
+    pentadsolver_handle_t handle, int elem_bytes, const void *ds, const void *dl,
+    const void *d, const void *du, const void *dw, void *x, void *x_save, const int *t_dims,
+    int t_ndim, int t_solvedim, void *t_buffer, size_t t_buffer_bytes, int reps, void *stream,
+    char *report, size_t report_len);
 
 /* No counterpart in the reference.  An FP64 solve that allocates nothing and
  * takes no scratch buffer, for callers that cannot call cudaMalloc around a

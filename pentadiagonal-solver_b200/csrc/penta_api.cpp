@@ -87,6 +87,21 @@ Knobs knobs_from(const std::string &tuning) {
   return k;
 }
 
+// Does the environment fix the kernel choice of this direction (the algorithm
+// selectors, PENTA_PCR_LANES, or a kernel knob)?  Then the tuning table is
+// not consulted, as the reference's selectors win over everything.
+bool env_fixes_choice(int dir) {
+  auto set = [](const char *name) {
+    const char *v = std::getenv(name);
+    return v != nullptr && v[0] != '\0';
+  };
+  if (dir == 0 ? set("PENTA_XALGO")
+               : (set(dir == 1 ? "PENTA_YALGO" : "PENTA_ZALGO") || set("PENTA_YZALGO")))
+    return true;
+  return set("PENTA_PCR_LANES") || env_flag("PENTA_NO_TMA") || env_flag("PENTA_NO_TMEM") ||
+         set("PENTA_TMEM_VARIANT") || set("PENTA_TMA_VARIANT");
+}
+
 // ---------------------------------------------------------------------------
 // Contexts
 // ---------------------------------------------------------------------------
@@ -102,6 +117,7 @@ struct Context {
   std::string variant[3];
   std::string tuning[3];  // pentadsolver_set_tuning, per direction ("" = none)
   std::unordered_map<long long, int> occ_cache;  // (variant, n) -> CTAs/SM
+  std::string gpu_name;  // the device's name (tuning-table keys)
   cudaStream_t copy_stream = nullptr;  // non-blocking: plan-table uploads (copy_h2d)
 
   bool init() {  // idempotent; needs a usable device
@@ -119,6 +135,12 @@ struct Context {
       cudaGetLastError();
       return false;
     }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    gpu_name = prop.name;
     sm_count = sms;
     smem_optin = optin;
     device = dev;
@@ -487,12 +509,25 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
   SolveArgs<F> a{ds, dl, d, du, dw, x, sh.L, buf, buf_bytes, status_word};
   const int dir = sh.dir;
   const bool contig = (dir == 0);
-  const Algo want = selected_algo(ctx, dir);
-  const int lanes = selected_lanes(ctx, dir);
+  Algo want = selected_algo(ctx, dir);
+  int lanes = selected_lanes(ctx, dir);
   Knobs kn;
+  bool open_choice;
   {
     std::lock_guard<std::mutex> lock(ctx.mu);
     kn = knobs_from(ctx.tuning[dir]);
+    open_choice = ctx.tuning[dir].empty() && ctx.forced[dir] == Algo::Auto &&
+                  ctx.forced_lanes[dir] == 0;
+  }
+  // the tuning table decides what neither the environment nor the handle fixes
+  if (open_choice && !tune_table_empty() && !env_fixes_choice(dir)) {
+    TuneChoice tc;
+    if (tune_lookup(tune_key(ctx.gpu_name, "solve", sizeof(F), dir, sh.L.n, sh.L.n_sys), tc)) {
+      kn = knobs_from(tc.spec.empty() ? std::string("auto") : tc.spec);
+      const Algo ta = parse_algo(tc.algo.c_str());
+      want = ta == Algo::Unknown ? Algo::Auto : ta;
+      lanes = tc.lanes;
+    }
   }
   const bool debug = env_flag("PENTA_DEBUG_LAUNCH");
 
@@ -687,6 +722,7 @@ struct PlanSingle {  // a grid the batched kernel does not take: solved alone
 struct Plan {
   Context *ctx = nullptr;
   int slot = 0;  // status word slot of this plan
+  std::string tkey;  // its tuning-table key (longest line, all lines)
   int elem = 8, solvedim = 0;
   bool contig = false, w2s = false, discard = false;
   unsigned char *table = nullptr, *scratch = nullptr;
@@ -881,6 +917,20 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
   p->n_jobs = (int)order.size();
   p->total_tiles = total_tiles;
   p->groups = groups;
+  {
+    long long max_n = 0, lines = 0;
+    for (int i : order) {
+      Shape sh;
+      make_shape(grids[i].dims, grids[i].ndim, solvedim, sh, why);
+      max_n = std::max(max_n, sh.L.n);
+      lines += sh.L.n_sys;
+    }
+    p->tkey = tune_key(ctx.gpu_name, "plan", sizeof(F), contig ? 0 : 1, max_n, lines);
+  }
+  if (ctas == 0) {  // the tuning table's CTA count for plans of this class
+    TuneChoice tc;
+    if (tune_lookup(p->tkey, tc) && tc.ctas > 0) ctas = tc.ctas;
+  }
   p->ctas = (ctas > 0 && ctas < ctx.sm_count) ? ctas : ctx.sm_count;
   p->singles = singles;
   char d[160];
@@ -1046,6 +1096,130 @@ void refine_fp32_grids(int count, const pentadsolver_grid_t *grids,
     out[i].dw = s + 4 * N;
     out[i].x = r;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Autotuning of single solves
+// ---------------------------------------------------------------------------
+struct TuneCandidate {
+  const char *label, *spec, *algo;
+  int lanes;
+};
+// Tensor-Memory kernel variants (forward ring and read-back stages), the older
+// TMA kernels, the cp.async kernel with two lanes or one lane per line.
+constexpr TuneCandidate kTuneCandidates[] = {
+    {"tmem 2/4", "tmem=2,4", "thomas-pcr", 2}, {"tmem 2/3", "tmem=2,3", "thomas-pcr", 2},
+    {"tmem 3/4", "tmem=3,4", "thomas-pcr", 2}, {"tmem 3/3", "tmem=3,3", "thomas-pcr", 2},
+    {"tmem 3/2", "tmem=3,2", "thomas-pcr", 2}, {"tmem 4/3", "tmem=4,3", "thomas-pcr", 2},
+    {"tma", "no-tmem", "thomas-pcr", 2},       {"cp.async P2", "no-tma", "thomas-pcr", 2},
+    {"cp.async P1", "no-tma", "thomas-pcr", 1},
+};
+
+// Times every candidate on the caller's problem (x is overwritten by the
+// trials; x_save, when given, keeps and restores it), records the fastest in
+// the tuning table and writes a report: one line per distinct kernel variant,
+// "label\tspec\talgo\tlanes\tvariant\tms", the fastest first.
+template <typename F>
+pentadStatus_t autotune_solve(Context &ctx, const F *ds, const F *dl, const F *d, const F *du,
+                              const F *dw, F *x, F *x_save, const int *dims, int ndim,
+                              int solvedim, void *buf, size_t buf_bytes, int reps,
+                              cudaStream_t stream, std::string &report, const char **why) {
+  Shape sh;
+  pentadStatus_t st = make_shape(dims, ndim, solvedim, sh, why);
+  if (st != PENTAD_STATUS_SUCCESS) return st;
+  if (reps < 1 || reps > 1000) {
+    *why = "reps out of range";
+    return PENTAD_STATUS_INVALID_VALUE;
+  }
+  if (!ctx.init()) {
+    *why = "no usable CUDA device";
+    return PENTAD_STATUS_NOT_INITIALIZED;
+  }
+  if (!on_own_device(ctx, why)) return PENTAD_STATUS_INVALID_VALUE;
+  const size_t bytes = (size_t)sh.L.n * (size_t)sh.L.n_sys * sizeof(F);
+  if (x_save != nullptr &&
+      cudaMemcpyAsync(x_save, x, bytes, cudaMemcpyDeviceToDevice, stream) != cudaSuccess) {
+    cudaGetLastError();
+    return PENTAD_STATUS_EXECUTION_FAILED;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    if (e0) cudaEventDestroy(e0);
+    return PENTAD_STATUS_EXECUTION_FAILED;
+  }
+  const int dir = sh.dir;
+  struct Row {
+    const TuneCandidate *c;
+    std::string variant;
+    float ms;
+  };
+  std::vector<Row> rows;
+  std::unordered_set<std::string> seen;
+  pentadStatus_t out = PENTAD_STATUS_SUCCESS;
+  for (const TuneCandidate &c : kTuneCandidates) {
+    Context trial;
+    trial.init();
+    trial.slot = ctx.slot;
+    trial.tuning[dir] = c.spec;
+    trial.forced[dir] = parse_algo(c.algo);
+    trial.forced_lanes[dir] = c.lanes;
+    const char *w = "";
+    if (solve<F>(trial, ds, dl, d, du, dw, x, dims, ndim, solvedim, buf, buf_bytes, stream,
+                 &w) != PENTAD_STATUS_SUCCESS) {
+      cudaGetLastError();
+      continue;
+    }
+    const std::string variant = trial.variant[dir];
+    if (!seen.insert(variant).second) continue;  // the shape sent it to a kernel timed already
+    bool ok = cudaEventRecord(e0, stream) == cudaSuccess;
+    for (int r = 0; ok && r < reps; ++r)
+      ok = solve<F>(trial, ds, dl, d, du, dw, x, dims, ndim, solvedim, buf, buf_bytes, stream,
+                    &w) == PENTAD_STATUS_SUCCESS;
+    float ms = 0.f;
+    ok = ok && cudaEventRecord(e1, stream) == cudaSuccess &&
+         cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      out = PENTAD_STATUS_EXECUTION_FAILED;
+      break;
+    }
+    rows.push_back(Row{&c, variant, ms / reps});
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (x_save != nullptr &&
+      cudaMemcpyAsync(x, x_save, bytes, cudaMemcpyDeviceToDevice, stream) != cudaSuccess) {
+    cudaGetLastError();
+    out = PENTAD_STATUS_EXECUTION_FAILED;
+  }
+  if (out != PENTAD_STATUS_SUCCESS) return out;
+  if (rows.empty()) {
+    *why = "no candidate ran";
+    return PENTAD_STATUS_EXECUTION_FAILED;
+  }
+  std::stable_sort(rows.begin(), rows.end(), [](const Row &a, const Row &b) { return a.ms < b.ms; });
+  TuneChoice best;
+  best.spec = rows[0].c->spec;
+  best.algo = rows[0].c->algo;
+  best.lanes = rows[0].c->lanes;
+  best.ms = rows[0].ms;
+  tune_store(tune_key(ctx.gpu_name, "solve", sizeof(F), dir, sh.L.n, sh.L.n_sys), best);
+  report.clear();
+  for (const Row &r : rows) {
+    char ms[32];
+    std::snprintf(ms, sizeof ms, "%.6g", r.ms);
+    report += std::string(r.c->label) + "\t" + r.c->spec + "\t" + r.c->algo + "\t" +
+              std::to_string(r.c->lanes) + "\t" + r.variant + "\t" + ms + "\n";
+  }
+  return PENTAD_STATUS_SUCCESS;
+}
+
+bool copy_out(const std::string &v, char *out, size_t len) {
+  if (out == nullptr || len == 0) return out == nullptr;
+  if (v.size() + 1 > len) return false;
+  std::memcpy(out, v.c_str(), v.size() + 1);
+  return true;
 }
 
 // Read and clear one status slot; ZERO_PIVOT when bit 0 was set.
@@ -1569,6 +1743,17 @@ extern "C" pentadStatus_t pentadsolver_refine_plan_create(pentadsolver_handle_t 
   size_t tb = 0, sb = 0;
   st = pentadsolver_plan_sizes(h, 4, count, g32.data(), solvedim, &tb, &sb);
   if (st != PENTAD_STATUS_SUCCESS) return st;
+  std::string rkey;
+  {
+    long long max_n = 0, lines = 0;
+    for (const penta::Shape &sh : shapes) {
+      max_n = std::max(max_n, sh.L.n);
+      lines += sh.L.n_sys;
+    }
+    rkey = penta::tune_key(ctx->gpu_name, "refine", 8, solvedim == 0 ? 0 : 1, max_n, lines);
+    penta::TuneChoice tc;
+    if (ctas == 0 && penta::tune_lookup(rkey, tc) && tc.ctas > 0) ctas = tc.ctas;
+  }
   st = penta::plan_build<float>(*ctx, count, g32.data(), solvedim, base + fp32_off, tb,
                                 base + fp32_off + tb, buffer_bytes - fp32_off - tb, ctas, fp32,
                                 &why);
@@ -1610,6 +1795,7 @@ extern "C" pentadStatus_t pentadsolver_refine_plan_create(pentadsolver_handle_t 
   p->est = est;
   p->count = count;
   p->fp32 = fp32;
+  p->tkey = rkey;
   p->desc = "refine steps=" + std::to_string(steps) + " over " + fp32->desc;
   *plan = new pentadsolver_plan_s{p};
   return PENTAD_STATUS_SUCCESS;
@@ -1626,5 +1812,165 @@ extern "C" pentadStatus_t pentadsolver_plan_estimates(pentadsolver_plan_t plan, 
     cudaGetLastError();
     return PENTAD_STATUS_EXECUTION_FAILED;
   }
+  return PENTAD_STATUS_SUCCESS;
+}
+
+// ===========================================================================
+// Tuning table and autotuning (pentadsolver_ext.h)
+// ===========================================================================
+extern "C" pentadStatus_t pentadsolver_tuning_load(const char *path) {
+  if (path == nullptr) return PENTAD_STATUS_INVALID_VALUE;
+  return penta::tune_load(path) ? PENTAD_STATUS_SUCCESS : PENTAD_STATUS_INVALID_VALUE;
+}
+
+extern "C" pentadStatus_t pentadsolver_tuning_save(const char *path) {
+  if (path == nullptr) return PENTAD_STATUS_INVALID_VALUE;
+  return penta::tune_save(path) ? PENTAD_STATUS_SUCCESS : PENTAD_STATUS_INVALID_VALUE;
+}
+
+extern "C" pentadStatus_t pentadsolver_tuning_clear(void) {
+  penta::tune_clear();
+  return PENTAD_STATUS_SUCCESS;
+}
+
+extern "C" pentadStatus_t pentadsolver_tuning_set(const char *key, const char *spec,
+                                                  const char *algo, int lanes, int ctas,
+                                                  double ms) {
+  if (key == nullptr || key[0] == '\0' || lanes < 0 || lanes > 32 || ctas < 0)
+    return PENTAD_STATUS_INVALID_VALUE;
+  std::string sp = spec ? spec : "";
+  if (sp == "auto") sp.clear();
+  if (!(sp.empty() || sp == "no-tma" || sp == "no-tmem" || sp.rfind("tmem=", 0) == 0 ||
+        sp.rfind("tma=", 0) == 0))
+    return PENTAD_STATUS_INVALID_VALUE;
+  std::string al = algo ? algo : "";
+  if (al == "auto") al.clear();
+  if (!al.empty() && penta::parse_algo(al.c_str()) == penta::Algo::Unknown)
+    return PENTAD_STATUS_INVALID_VALUE;
+  penta::TuneChoice c;
+  c.spec = sp;
+  c.algo = al;
+  c.lanes = lanes;
+  c.ctas = ctas;
+  c.ms = ms;
+  penta::tune_store(key, c);
+  return PENTAD_STATUS_SUCCESS;
+}
+
+extern "C" pentadStatus_t pentadsolver_tuning_lookup(const char *key, char *out, size_t len) {
+  if (key == nullptr) return PENTAD_STATUS_INVALID_VALUE;
+  penta::TuneChoice c;
+  if (!penta::tune_lookup(key, c)) return PENTAD_STATUS_INVALID_VALUE;
+  return penta::copy_out(penta::tune_format(c), out, len) ? PENTAD_STATUS_SUCCESS
+                                                          : PENTAD_STATUS_INVALID_VALUE;
+}
+
+extern "C" pentadStatus_t pentadsolver_tuning_key(const char *gpu_name, const char *kind,
+                                                  int elem_bytes, const int *dims, int ndim,
+                                                  int solvedim, char *out, size_t len) {
+  if (kind == nullptr || (std::strcmp(kind, "solve") && std::strcmp(kind, "plan") &&
+                          std::strcmp(kind, "refine")) ||
+      (elem_bytes != 4 && elem_bytes != 8))
+    return PENTAD_STATUS_INVALID_VALUE;
+  penta::Shape sh;
+  const char *why = "";
+  pentadStatus_t st = penta::make_shape(dims, ndim, solvedim, sh, &why);
+  if (st != PENTAD_STATUS_SUCCESS) return st;
+  std::string gpu;
+  if (gpu_name != nullptr) {
+    gpu = gpu_name;
+  } else {
+    Context *ctx = penta::resolve(nullptr);
+    if (!ctx->init()) return PENTAD_STATUS_NOT_INITIALIZED;
+    gpu = ctx->gpu_name;
+  }
+  const int dir = std::strcmp(kind, "solve") ? (solvedim == 0 ? 0 : 1) : sh.dir;
+  return penta::copy_out(penta::tune_key(gpu, kind, (size_t)elem_bytes, dir, sh.L.n, sh.L.n_sys),
+                         out, len)
+             ? PENTAD_STATUS_SUCCESS
+             : PENTAD_STATUS_INVALID_VALUE;
+}
+
+extern "C" pentadStatus_t pentadsolver_autotune_solve(
+    pentadsolver_handle_t h, int elem_bytes, const void *ds, const void *dl, const void *d,
+    const void *du, const void *dw, void *x, void *x_save, const int *t_dims, int t_ndim,
+    int t_solvedim, void *t_buffer, size_t t_buffer_bytes, int reps, void *stream,
+    char *report, size_t report_len) {
+  if ((elem_bytes != 4 && elem_bytes != 8) || !ds || !dl || !d || !du || !dw || !x)
+    return PENTAD_STATUS_INVALID_VALUE;
+  Context *ctx = penta::resolve(h);
+  const char *why = "";
+  std::string rep;
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  pentadStatus_t st =
+      elem_bytes == 8
+          ? penta::autotune_solve<double>(
+                *ctx, static_cast<const double *>(ds), static_cast<const double *>(dl),
+                static_cast<const double *>(d), static_cast<const double *>(du),
+                static_cast<const double *>(dw), static_cast<double *>(x),
+                static_cast<double *>(x_save), t_dims, t_ndim, t_solvedim, t_buffer,
+                t_buffer_bytes, reps, s, rep, &why)
+          : penta::autotune_solve<float>(
+                *ctx, static_cast<const float *>(ds), static_cast<const float *>(dl),
+                static_cast<const float *>(d), static_cast<const float *>(du),
+                static_cast<const float *>(dw), static_cast<float *>(x),
+                static_cast<float *>(x_save), t_dims, t_ndim, t_solvedim, t_buffer,
+                t_buffer_bytes, reps, s, rep, &why);
+  if (st != PENTAD_STATUS_SUCCESS) {
+    if (penta::env_flag("PENTA_DEBUG_LAUNCH")) std::fprintf(stderr, "[penta] autotune: %s\n", why);
+    return st;
+  }
+  return penta::copy_out(rep, report, report_len) ? PENTAD_STATUS_SUCCESS
+                                                  : PENTAD_STATUS_INVALID_VALUE;
+}
+
+extern "C" pentadStatus_t pentadsolver_autotune_plan(pentadsolver_plan_t plan, int reps,
+                                                     void *stream, int *best_ctas) {
+  if (plan == nullptr || plan->p == nullptr || reps < 1 || reps > 1000)
+    return PENTAD_STATUS_INVALID_VALUE;
+  penta::Plan &p = *plan->p;
+  Context &ctx = *p.ctx;
+  const char *why = "";
+  if (!penta::on_own_device(ctx, &why)) return PENTAD_STATUS_INVALID_VALUE;
+  penta::Plan &launching = p.fp32 ? *p.fp32 : p;  // whose ctas the launches use
+  const int before = launching.ctas;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    if (e0) cudaEventDestroy(e0);
+    return PENTAD_STATUS_EXECUTION_FAILED;
+  }
+  static constexpr double kFractions[] = {1.0, 0.9, 0.75, 0.5};
+  int best = before;
+  float best_ms = -1.f;
+  pentadStatus_t st = PENTAD_STATUS_SUCCESS;
+  for (double f : kFractions) {
+    launching.ctas = std::max(1, (int)(ctx.sm_count * f));
+    if ((st = pentadsolver_plan_execute(plan, stream)) != PENTAD_STATUS_SUCCESS) break;  // warm-up
+    bool ok = cudaEventRecord(e0, static_cast<cudaStream_t>(stream)) == cudaSuccess;
+    for (int r = 0; ok && r < reps; ++r) ok = pentadsolver_plan_execute(plan, stream) == PENTAD_STATUS_SUCCESS;
+    float ms = 0.f;
+    ok = ok && cudaEventRecord(e1, static_cast<cudaStream_t>(stream)) == cudaSuccess &&
+         cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      st = PENTAD_STATUS_EXECUTION_FAILED;
+      break;
+    }
+    ms /= reps;
+    if (best_ms < 0.f || ms < best_ms) {
+      best_ms = ms;
+      best = launching.ctas;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  launching.ctas = st == PENTAD_STATUS_SUCCESS ? best : before;
+  if (st != PENTAD_STATUS_SUCCESS) return st;
+  penta::TuneChoice c;
+  c.ctas = best;
+  c.ms = best_ms;
+  penta::tune_store(p.tkey, c);
+  if (best_ctas) *best_ctas = best;
   return PENTAD_STATUS_SUCCESS;
 }

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime_api.h>
 #include <cstddef>
+#include <string>
 #include <type_traits>
 #include <vector>
 
@@ -154,6 +155,25 @@ enum class RefineStep { PrepareCast, Prepare, Lift, Residual, Correct };
 int refine_chunks(long long n_points);
 cudaError_t launch_refine_step(RefineStep step, const RefineGrid &one, const RefineGrid *table,
                                int count, int total_chunks, cudaStream_t stream);
+
+// penta_tune.cpp: the process-wide tuning table (an autotuner's measured
+// choices per shape class; read from PENTA_TUNING_CACHE on first use).
+struct TuneChoice {
+  std::string spec;  // pentadsolver_set_tuning string ("" = automatic)
+  std::string algo;  // kernel family ("thomas-pcr", ...; "" = automatic)
+  int lanes = 0;     // PCR lanes (0 = automatic)
+  int ctas = 0;      // a plan's CTA count (0 = every SM)
+  double ms = 0.0;   // the measured time
+};
+std::string tune_key(const std::string &gpu, const char *kind, size_t elem, int dir,
+                     long long n, long long lines);
+bool tune_lookup(const std::string &key, TuneChoice &out);
+bool tune_table_empty();
+void tune_store(const std::string &key, const TuneChoice &c);
+bool tune_load(const char *path);
+bool tune_save(const char *path);
+void tune_clear();
+std::string tune_format(const TuneChoice &c);  // "spec\talgo\tlanes\tctas\tms"
 
 // penta_status.cu: status words, one slot per handle or plan in a fixed
 // device array (slot 0: the handle-less calls).  Addresses are taken with

@@ -386,6 +386,16 @@ class Plan:
     def describe(self) -> str:
         return _typed("pentadsolver_plan_describe", [_P], ctypes.c_char_p)(self._plan).decode()
 
+    def autotune(self, reps: int = 5, stream=None) -> int:
+        """Time executes at several CTA counts, keep the fastest for this plan
+        and record it in the library's tuning table; returns the CTA count."""
+        best = ctypes.c_int(0)
+        st = _typed("pentadsolver_autotune_plan", [_P, _I, _P, ctypes.POINTER(_I)])(
+            self._plan, int(reps), _stream_ptr(stream, self.device), ctypes.byref(best))
+        if st != SUCCESS:
+            raise PentadError(st, "plan autotune")
+        return int(best.value)
+
     def status_check(self, stream=None) -> tuple[int, int]:
         """Read and clear this plan's own status bits, then synchronise."""
         bits = ctypes.c_int(0)
@@ -495,3 +505,80 @@ def aligned_bytes(n: int, device="cuda"):
     raw = torch.empty(n + 256, dtype=torch.uint8, device=device)
     off = (-raw.data_ptr()) % 256
     return raw[off:off + n]
+
+
+# ---------------------------------------------------------------------------
+# The library's tuning table and autotuner
+# ---------------------------------------------------------------------------
+def tuning_load(path) -> None:
+    st = _typed("pentadsolver_tuning_load", [ctypes.c_char_p])(os.fsencode(str(path)))
+    if st != SUCCESS:
+        raise PentadError(st, f"tuning_load {path}")
+
+
+def tuning_save(path) -> None:
+    st = _typed("pentadsolver_tuning_save", [ctypes.c_char_p])(os.fsencode(str(path)))
+    if st != SUCCESS:
+        raise PentadError(st, f"tuning_save {path}")
+
+
+def tuning_clear() -> None:
+    _typed("pentadsolver_tuning_clear", [])()
+
+
+def tuning_set(key: str, spec: str = "auto", algo: str = "auto", lanes: int = 0, ctas: int = 0,
+               ms: float = 0.0) -> None:
+    st = _typed("pentadsolver_tuning_set",
+                [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _I, _I, ctypes.c_double])(
+        key.encode(), spec.encode(), algo.encode(), int(lanes), int(ctas), float(ms))
+    if st != SUCCESS:
+        raise PentadError(st, "tuning_set")
+
+
+def tuning_lookup(key: str) -> dict | None:
+    """The table's entry for ``key`` (spec, algo, lanes, ctas, ms), or None."""
+    out = ctypes.create_string_buffer(512)
+    st = _typed("pentadsolver_tuning_lookup", [ctypes.c_char_p, ctypes.c_char_p, _Z])(
+        key.encode(), out, 512)
+    if st != SUCCESS:
+        return None
+    spec, algo, lanes, ctas, ms = out.value.decode().split("\t")
+    return {"spec": spec, "algo": algo, "lanes": int(lanes), "ctas": int(ctas), "ms": float(ms)}
+
+
+def tuning_key(dims, solvedim: int, elem_bytes: int = 8, kind: str = "solve",
+               gpu_name: str | None = None) -> str:
+    out = ctypes.create_string_buffer(512)
+    st = _typed("pentadsolver_tuning_key",
+                [ctypes.c_char_p, ctypes.c_char_p, _I, _P, _I, _I, ctypes.c_char_p, _Z])(
+        None if gpu_name is None else gpu_name.encode(), kind.encode(), int(elem_bytes),
+        _dims(dims), len(dims), int(solvedim), out, 512)
+    if st != SUCCESS:
+        raise PentadError(st, "tuning_key")
+    return out.value.decode()
+
+
+def autotune_solve(ds, dl, d, du, dw, x, solvedim: int, reps: int = 5, buffer=None,
+                   x_save=None, stream=None, handle=None) -> list[dict]:
+    """The library's autotuner on this problem: every distinct candidate's
+    time, fastest first (the first is now in the tuning table)."""
+    _check_arrays((ds, dl, d, du, dw, x))
+    pre, eb = _elem_prefix(x.dtype)
+    dims = dims_of(x)
+    if buffer is None:
+        buffer = alloc_buffer(dims, solvedim, x.dtype, x.device)
+    nbytes = buffer.numel() * buffer.element_size()
+    out = ctypes.create_string_buffer(8192)
+    st = _typed("pentadsolver_autotune_solve",
+                [_P, _I] + [_P] * 7 + [_P, _I, _I, _P, _Z, _I, _P, ctypes.c_char_p, _Z])(
+        _hval(handle), eb, *(_ptr(a) for a in (ds, dl, d, du, dw, x)),
+        None if x_save is None else _ptr(x_save), _dims(dims), len(dims), int(solvedim),
+        _ptr(buffer), nbytes, int(reps), _stream_ptr(stream, x.device), out, 8192)
+    if st != SUCCESS:
+        raise PentadError(st, "autotune_solve")
+    rows = []
+    for line in out.value.decode().splitlines():
+        label, spec, algo, lanes, variant, ms = line.split("\t")
+        rows.append({"label": label, "spec": spec, "algo": algo, "lanes": int(lanes),
+                     "variant": variant, "ms": float(ms)})
+    return rows
