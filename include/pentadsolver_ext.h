@@ -217,6 +217,28 @@ EXTERN_C PENTAD_API pentadStatus_t pentadsolver_autotune_solve(
     int t_ndim, int t_solvedim, void *t_buffer, size_t t_buffer_bytes, int reps, void *stream,
     char *report, size_t report_len);
 
+/* ---- Slab decomposition over several GPUs ----------------------------------
+ * The multi-GPU form of the ADI sweep.  The reference distributes one solve
+ * direction over MPI ranks and exchanges a reduced system through host memory
+ * (src/cuda/mpi/pentad_cuda.cu:929-955, :529-555); here a grid of
+ * nx x ny x nz points (x contiguous) is split into `parts` slabs along z, one
+ * per GPU: x and y lines lie inside a slab and are solved in place, and one
+ * all-to-all of equal blocks turns the z slabs into y slabs (rank r: y in
+ * [r ny/parts, (r+1) ny/parts), all z, as [z][y][x]) in which z lines are
+ * local, and back.  These two kernels are the data movement around that
+ * exchange: pack gathers, for every destination rank r, the rank's block
+ * send[r][zl][yl][x] = zslab[zl][r ny/parts + yl][x] (the all-to-all's
+ * receive buffer is then the y slab itself); unpack scatters what the way
+ * back receives, recv[r][zl][yl][x], into the z slab.  nz_local is the slab's
+ * own z extent; ny must be a multiple of parts.  Asynchronous on `stream`. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_slab_pack(int elem_bytes, const void *zslab,
+                                                          void *send, int nx, int ny,
+                                                          int nz_local, int parts, void *stream);
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_slab_unpack(int elem_bytes, const void *recv,
+                                                            void *zslab, int nx, int ny,
+                                                            int nz_local, int parts,
+                                                            void *stream);
+
 /* No counterpart in the reference.  An FP64 solve that allocates nothing and
  * takes no scratch buffer, for callers that cannot call cudaMalloc around a
  * solve: applications whose device memory is all owned by their own pool,

@@ -156,6 +156,12 @@ int refine_chunks(long long n_points);
 cudaError_t launch_refine_step(RefineStep step, const RefineGrid &one, const RefineGrid *table,
                                int count, int total_chunks, cudaStream_t stream);
 
+// slab_kernels.cu: the segment copies of the slab-decomposed ADI (pack: the
+// z-slab's blocks for every destination rank into one buffer; unpack: back).
+cudaError_t launch_slab_copy(int elem_bytes, const void *src, void *dst, int nx, int ny,
+                             int nz_local, int parts, bool to_packed, int sm_count,
+                             cudaStream_t stream);
+
 // penta_tune.cpp: the process-wide tuning table (an autotuner's measured
 // choices per shape class; read from PENTA_TUNING_CACHE on first use).
 struct TuneChoice {

@@ -582,3 +582,26 @@ def autotune_solve(ds, dl, d, du, dw, x, solvedim: int, reps: int = 5, buffer=No
         rows.append({"label": label, "spec": spec, "algo": algo, "lanes": int(lanes),
                      "variant": variant, "ms": float(ms)})
     return rows
+
+
+# ---------------------------------------------------------------------------
+# Slab decomposition (the data movement around the all-to-all)
+# ---------------------------------------------------------------------------
+def _slab_call(name, elem_bytes, src, dst, nx, ny, nz_local, parts, stream):
+    sp = None
+    if stream is not None:
+        sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+    return int(_typed(name, [_I, _P, _P, _I, _I, _I, _I, _P])(
+        int(elem_bytes), _ptr(src), _ptr(dst), int(nx), int(ny), int(nz_local), int(parts), sp))
+
+
+def slab_pack(elem_bytes, zslab, send, nx, ny, nz_local, parts, stream=None) -> int:
+    """send[r][zl][yl][x] = zslab[zl][r ny/parts + yl][x] (pentadsolver_slab_pack)."""
+    return _slab_call("pentadsolver_slab_pack", elem_bytes, zslab, send, nx, ny, nz_local,
+                      parts, stream)
+
+
+def slab_unpack(elem_bytes, recv, zslab, nx, ny, nz_local, parts, stream=None) -> int:
+    """zslab[zl][r ny/parts + yl][x] = recv[r][zl][yl][x] (pentadsolver_slab_unpack)."""
+    return _slab_call("pentadsolver_slab_unpack", elem_bytes, recv, zslab, nx, ny, nz_local,
+                      parts, stream)
