@@ -16,7 +16,9 @@
            N ~ logU[16, 512] from a device-resident pool, solvedim U{0,1,2},
            70% at tolerance 1e-10 and 30% at 1e-13, 150 GB budget; p50/p99
            latency and solves/s for the mixed and FP64 policies and for
-           sequential plain FP64 calls, at that rate and at saturation.
+           sequential plain FP64 calls, at that rate and at saturation; the
+           mixed policy first measures, per solve direction, whether the
+           refined form beats plain FP64 and uses it only where it does.
 
   mesh     the reference's random benchmark grid, 256^3 FP64 (the largest of
            benchmarks/cuda/my_bm.cu), built on the device by
@@ -364,7 +366,7 @@ def config4(rate=2000.0, seconds=2.0, n_problems=64, budget=150e9, seed=44):
                                    seed=seed + 1)
         res = {}
         for policy in ("mixed", "fp64", "sequential"):
-            rep, ex, _ = serving.serve(pool, trace, policy, budget)
+            rep, ex, _ = serving.serve(pool, trace, policy, budget, calibrate=True)
             res[policy] = rep
             del ex
             torch.cuda.empty_cache()

@@ -17,7 +17,12 @@ a Poisson stream in the benchmarks.  The loop
 
 Precision classes: requests at tolerance >= 1e-10 may use mixed precision
 (FP32 sweeps + FP64 refinement) under the "mixed" policy; tighter ones always
-use plain FP64.  The "sequential" policy is the baseline: each request solved
+use plain FP64.  The mixed policy takes the refined form only where it pays:
+the executor measures, per solve direction, a refinement plan against a
+plain FP64 plan on the pool's largest problem at start-up, and loose
+requests of a direction whose refined form measured slower run in FP64.  (On
+a part whose FP64 sweep is bandwidth-bound, as on B200, that is every
+direction: the refined form moves more bytes per point than plain FP64.)  The "sequential" policy is the baseline: each request solved
 alone by one plain FP64 call, in arrival order.
 
 The scheduler (admission, grouping, budget accounting) is independent of the
@@ -114,8 +119,10 @@ class Scheduler:
     def key_of(self, r: Request):
         if self.policy == "sequential":
             return ("seq", r.rid)
-        prec = "mixed" if (self.policy == "mixed" and r.mixed_ok) else "f64"
-        return (r.solvedim, prec)
+        refine_pays = getattr(self.x, "refine_pays", None)
+        mixed = (self.policy == "mixed" and r.mixed_ok and
+                 (refine_pays is None or refine_pays(r.solvedim)))
+        return (r.solvedim, "mixed" if mixed else "f64")
 
     def run(self, trace: list[Request]) -> list[Request]:
         pending = sorted(trace, key=lambda r: r.arrival)
@@ -223,7 +230,7 @@ class CudaExecutor:
     """Runs batches as plans (or, for the sequential baseline, single calls)."""
 
     def __init__(self, pool: ProblemPool, refine_steps: int = 1, streams: int = 3,
-                 keep_results: bool = False):
+                 keep_results: bool = False, calibrate: bool = False):
         import torch
 
         import pentadsolver as ps
@@ -239,6 +246,42 @@ class CudaExecutor:
         self.status = {}   # request id -> status bits of the batch that solved it
         self.t0 = time.perf_counter()
         self.handle = ps.Handle()
+        # per solve direction: does the refined form beat plain FP64 here?
+        self.calibration = self.measure_costs() if calibrate else None
+
+    def measure_costs(self, reps: int = 3) -> dict:
+        """Time a refinement plan against a plain FP64 plan along each solve
+        direction on the pool's largest problem (device time, after a warm-up
+        execute); the refined form is used only where it was faster."""
+        torch, ps = self.torch, self.ps
+        big = max(range(len(self.pool.shapes)), key=self.pool.points)
+        p = self.pool.items[big]
+        out = {}
+        for solvedim in range(3):
+            g = {"ds": p["ds"], "dl": p["dl"], "d": p["d"], "du": p["du"], "dw": p["dw"],
+                 "x": p["b"].clone()}
+            ms = {}
+            for label, steps in (("fp64", None), ("refined", self.refine_steps)):
+                with ps.Plan([g], solvedim, refine_steps=steps, handle=self.handle) as plan:
+                    plan.execute()
+                    torch.cuda.synchronize()
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    for _ in range(reps):
+                        plan.execute()
+                    e1.record()
+                    torch.cuda.synchronize()
+                    ms[label] = e0.elapsed_time(e1) / reps
+            out[solvedim] = {"fp64_ms": round(ms["fp64"], 4),
+                             "refined_ms": round(ms["refined"], 4),
+                             "refine_pays": ms["refined"] < ms["fp64"]}
+        return {"problem": list(self.pool.shapes[big]), "per_solvedim": out}
+
+    def refine_pays(self, solvedim: int) -> bool:
+        if self.calibration is None:
+            return True
+        return self.calibration["per_solvedim"][solvedim]["refine_pays"]
 
     def now(self) -> float:
         return time.perf_counter() - self.t0
@@ -312,12 +355,14 @@ class CudaExecutor:
 
 
 def serve(pool: ProblemPool, trace, policy: str, budget_bytes: float, max_batch: int = 64,
-          refine_steps: int = 1, keep_results: bool = False):
-    """Run a trace in real time; returns (report, executor)."""
+          refine_steps: int = 1, keep_results: bool = False, calibrate: bool = False):
+    """Run a trace in real time; returns (report, executor, trace).  With
+    `calibrate`, the mixed policy first measures where refinement pays."""
     import copy
 
     tr = copy.deepcopy(trace)
-    ex = CudaExecutor(pool, refine_steps=refine_steps, keep_results=keep_results)
+    ex = CudaExecutor(pool, refine_steps=refine_steps, keep_results=keep_results,
+                      calibrate=calibrate and policy == "mixed")
     sch = Scheduler(ex, budget_bytes, max_batch=max_batch,
                     max_in_flight=1 if policy == "sequential" else 3, policy=policy)
     ex.torch.cuda.synchronize()
@@ -327,4 +372,6 @@ def serve(pool: ProblemPool, trace, policy: str, budget_bytes: float, max_batch:
     rep = report(tr)
     rep.update({"policy": policy, "batches": sch.batches,
                 "peak_budget_gb": round(sch.peak / 1e9, 3)})
+    if ex.calibration is not None:
+        rep["calibration"] = ex.calibration
     return rep, ex, tr

@@ -95,3 +95,21 @@ def test_admission_waits_for_memory_and_keeps_arrival_order():
     assert starts == sorted(starts)
     assert sch.peak <= 8e6 + 24e6
     assert all(len(ids) == 1 for _, ids, _ in ex.log)
+
+
+def test_mixed_policy_routes_loose_requests_by_measured_cost():
+    # an executor that measured refinement slower along y only: loose y
+    # requests then join the FP64 batches, the others stay mixed
+    class Costed(FakeExecutor):
+        def refine_pays(self, solvedim):
+            return solvedim != 1
+
+    ex = Costed([1000] * 4)
+    sch = serving.Scheduler(ex, 1e12, policy="mixed")
+    loose = [serving.Request(i, 0.0, 0, d, 1e-10) for i, d in enumerate((0, 1, 2))]
+    tight = serving.Request(9, 0.0, 0, 1, 1e-13)
+    assert [sch.key_of(r) for r in loose] == [(0, "mixed"), (1, "f64"), (2, "mixed")]
+    assert sch.key_of(tight) == (1, "f64")
+    # without a measurement the loose requests are mixed
+    plain = serving.Scheduler(FakeExecutor([1000]), 1e12, policy="mixed")
+    assert plain.key_of(loose[1]) == (1, "mixed")
