@@ -20,6 +20,12 @@
            mixed policy first measures, per solve direction, whether the
            refined form beats plain FP64 and uses it only where it does.
 
+  odd      odd-size grids: each axis of 255^3 against 256^3, FP64 and FP32, timed as
+           single solves (CUDA events, 7 x 930 MB per axis: above L2, no flush),
+           with the misaligned rows / runs loaded by bulk copies (default) and
+           by element copies (PENTA_TMEM_LOADS=element), and the 16 smallest of
+           config 3's grids as FP64 plans; GB/s of 7 sizeof(F) B per point.
+
   mesh     the reference's random benchmark grid, 256^3 FP64 (the largest of
            benchmarks/cuda/my_bm.cu), built on the device by
            pentadsolver_D_mesh_random for several host thread counts, against
@@ -45,7 +51,7 @@ bench.py, this script uses oracle/ only as the checker (forward errors) and
 for the reference's own CPU code timed as the baseline; the solves and grids
 it measures are the library's.
 
-  python bench_configs.py [--configs 0,2,3,4,mesh,refapp]
+  python bench_configs.py [--configs 0,2,3,4,odd,mesh,refapp]
 """
 from __future__ import annotations
 
@@ -378,6 +384,66 @@ def config4(rate=2000.0, seconds=2.0, n_problems=64, budget=150e9, seed=44):
     return out
 
 
+def config_odd(reps=10):
+    import os
+
+    import torch
+
+    import pentadsolver as ps
+
+    out = {"config": "odd_sizes_single_solves", "rows": []}
+    pk = peak()
+    with ps.Handle() as h:
+        for dtype in (torch.float64, torch.float32):
+            eb = 8 if dtype == torch.float64 else 4
+            for edge in (256, 255):
+                dims = (edge, edge, edge)
+                p = dev_problem(dims, 7, dtype)
+                b = p["x"].clone()
+                for loads in ("", "element"):
+                    if loads and edge % (16 // eb) == 0:
+                        continue   # aligned: TMA tiles either way
+                    os.environ["PENTA_TMEM_LOADS"] = loads
+                    for axis in range(3):
+                        buf = ps.alloc_buffer(list(dims), axis, dtype)
+
+                        def run():
+                            ps.gpsv_batch(p["ds"], p["dl"], p["d"], p["du"], p["dw"], p["x"],
+                                          axis, buffer=buf, handle=h)
+
+                        ms = timed(run, reps=reps, warmup=2)
+                        p["x"].copy_(b)
+                        d = 0 if axis == 0 else (2 if axis == 2 else 1)
+                        gbs = 7 * eb * edge ** 3 / (ms * 1e-3) / 1e9
+                        out["rows"].append({"dtype": "f64" if eb == 8 else "f32", "edge": edge,
+                                            "axis": axis, "loads": loads or "default",
+                                            "variant": h.variant_that_ran(d),
+                                            "us": round(ms * 1e3, 1), "GBps": round(gbs, 1),
+                                            "frac": round(gbs / pk, 3)})
+                        del buf
+                    os.environ.pop("PENTA_TMEM_LOADS", None)
+                del p, b
+                torch.cuda.empty_cache()
+    # the 16 smallest grids of config 3 as FP64 plans (x, y, z), bulk and element loads
+    rng = np.random.default_rng(33)
+    dims_list = [tuple(int(v) for v in rng.integers(32, 385, size=3)) for _ in range(96)]
+    sub = sorted(dims_list, key=math.prod)[:16]
+    grids = [dev_problem(d, 500 + i) for i, d in enumerate(sub)]
+    pts = sum(math.prod(d) for d in sub)
+    for loads in ("", "element"):
+        os.environ["PENTA_TMEM_LOADS"] = loads
+        plans = [ps.Plan(grids, axis) for axis in range(3)]
+        ms = timed(lambda: [pl.execute() for pl in plans], reps=reps, warmup=2)
+        out[f"subset16_plans_{loads or 'default'}"] = {
+            "ms_xyz": round(ms, 3), "GBps": round(3 * 56 * pts / (ms * 1e-3) / 1e9, 1),
+            "plans": [pl.describe() for pl in plans]}
+        for pl in plans:
+            pl.close()
+        os.environ.pop("PENTA_TMEM_LOADS", None)
+    out["peak_GBps"] = pk
+    return out
+
+
 def config_mesh(edge=256):
     import torch
 
@@ -473,10 +539,10 @@ def main():
     want = {c.strip() for c in args.configs.split(",")}
     runs = {"0": config0, "2": lambda: config2(args.n2), "3": lambda: config3(args.grids3),
             "4": lambda: config4(seconds=args.seconds4), "mesh": config_mesh,
-            "refapp": config_refapp}
+            "refapp": config_refapp, "odd": config_odd}
     from bench import ClockSampler
 
-    for c in ("0", "2", "3", "4", "mesh", "refapp"):
+    for c in ("0", "2", "3", "4", "odd", "mesh", "refapp"):
         if c in want:
             t0 = time.time()
             with ClockSampler(0) as clk:
