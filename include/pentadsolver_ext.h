@@ -217,6 +217,60 @@ EXTERN_C PENTAD_API pentadStatus_t pentadsolver_autotune_solve(
     int t_ndim, int t_solvedim, void *t_buffer, size_t t_buffer_bytes, int reps, void *stream,
     char *report, size_t report_len);
 
+/* ---- Serving handle: a continuous-batching request loop -------------------
+ * No counterpart in the reference.  Requests -- one FP64 grid (the caller's
+ * device arrays; x is the right-hand side in and the solution out) and a
+ * solve direction, with the forward-error tolerance the caller needs -- are
+ * submitted as they arrive; pentadsolver_server_progress completes finished
+ * batches and launches new ones: the queued requests sharing the oldest
+ * one's solve direction and precision class, as one plan (one persistent
+ * launch), on the next of `n_streams` streams, while fewer than
+ * `max_in_flight` batches run -- so batches overlap and late arrivals join the
+ * next batch as memory frees.  All batch memory comes from `arena` (device
+ * memory, 256-byte aligned, the HBM budget); a batch that does not fit is
+ * shortened, and a request that alone exceeds the arena completes at once
+ * with PENTADSOLVER_SERVER_REJECTED_BIT.  Under PENTADSOLVER_SERVE_MIXED,
+ * requests with tol >= 1e-10 take FP32 sweeps + `refine_steps` FP64
+ * refinement steps along a direction where pentadsolver_server_calibrate
+ * measured that form faster than plain FP64 (everywhere if not measured);
+ * PENTADSOLVER_SERVE_SEQUENTIAL solves one request at a time (the baseline).
+ * Completed requests are read with pentadsolver_server_poll, each with the
+ * status bits of its batch (as pentadsolver_status_check reports them).
+ * Not thread-safe: drive one server from one thread. */
+typedef struct pentadsolver_server_s *pentadsolver_server_t;
+#define PENTADSOLVER_SERVE_FP64 0
+#define PENTADSOLVER_SERVE_MIXED 1
+#define PENTADSOLVER_SERVE_SEQUENTIAL 2
+#define PENTADSOLVER_SERVER_REJECTED_BIT (1 << 30)
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_server_create(
+    pentadsolver_handle_t handle, void *arena, size_t arena_bytes, int policy, int n_streams,
+    int max_batch, int max_in_flight, int refine_steps, pentadsolver_server_t *server);
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_server_submit(pentadsolver_server_t server,
+                                                              const pentadsolver_grid_t *grid,
+                                                              int solvedim, double tol,
+                                                              unsigned long long *id);
+/* wait = 0: complete what has finished and launch what fits, then return;
+ * wait = 1: run until every submitted request has completed. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_server_progress(pentadsolver_server_t server,
+                                                                int wait);
+/* Up to `capacity` completed requests: their ids and status bits. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_server_poll(pentadsolver_server_t server,
+                                                            unsigned long long *ids,
+                                                            int *bits, int capacity, int *n);
+/* out[0..count): queued, in flight, arena bytes used, arena peak, arena size,
+ * batches launched. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_server_stats(pentadsolver_server_t server,
+                                                             size_t *out, int count);
+/* Times a plain FP64 plan and a refinement plan of `sample` along each solve
+ * direction (`reps` executes each, the sample's x overwritten; arena memory,
+ * nothing in flight) and keeps, per direction, whether the refined form was
+ * faster; ms[2d], ms[2d + 1] receive the two times when ms is not NULL. */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_server_calibrate(pentadsolver_server_t server,
+                                                                 const pentadsolver_grid_t *sample,
+                                                                 int reps, double *ms);
+/* Waits for the batches in flight, then frees the server (not the arena). */
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_server_destroy(pentadsolver_server_t server);
+
 /* ---- Slab decomposition over several GPUs ----------------------------------
  * The multi-GPU form of the ADI sweep.  The reference distributes one solve
  * direction over MPI ranks and exchanges a reduced system through host memory

@@ -375,3 +375,167 @@ def serve(pool: ProblemPool, trace, policy: str, budget_bytes: float, max_batch:
     if ex.calibration is not None:
         rep["calibration"] = ex.calibration
     return rep, ex, tr
+
+
+# ---------------------------------------------------------------------------
+# The native serving handle (pentadsolver_server_*: admission, batching,
+# streams and memory in the library)
+# ---------------------------------------------------------------------------
+POLICIES = {"fp64": 0, "mixed": 1, "sequential": 2}
+
+
+class NativeServer:
+    """ctypes front end of the library's serving handle; its arena (the HBM
+    budget for batch memory) is one device allocation made here."""
+
+    def __init__(self, arena_bytes: int, policy: str = "fp64", streams: int = 3,
+                 max_batch: int = 64, max_in_flight: int = 3, refine_steps: int = 1,
+                 handle=None, device="cuda"):
+        import ctypes
+
+        import torch
+
+        import pentadsolver as ps
+
+        self.ps, self.ct = ps, ctypes
+        self.handle = handle
+        self.arena = torch.empty(int(arena_bytes) + 256, dtype=torch.uint8, device=device)
+        off = (-self.arena.data_ptr()) % 256
+        self._arena = self.arena[off:off + int(arena_bytes)]
+        self._srv = ctypes.c_void_p(None)
+        f = ps._typed("pentadsolver_server_create",
+                      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int,
+                       ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                       ctypes.POINTER(ctypes.c_void_p)])
+        st = f(ps._hval(handle), self._arena.data_ptr(), int(arena_bytes), POLICIES[policy],
+               int(streams), int(max_batch), int(max_in_flight), int(refine_steps),
+               ctypes.byref(self._srv))
+        if st != ps.SUCCESS:
+            raise ps.PentadError(st, "server create")
+        self._grids = {}   # id -> grid descriptor kept alive until completion
+
+    def submit(self, grid: dict, solvedim: int, tol: float) -> int:
+        ct, ps = self.ct, self.ps
+        desc = ps._grid_descs([grid])
+        rid = ct.c_ulonglong(0)
+        st = ps._typed("pentadsolver_server_submit",
+                       [ct.c_void_p, ct.POINTER(ps.GridDesc), ct.c_int, ct.c_double,
+                        ct.POINTER(ct.c_ulonglong)])(self._srv, desc, int(solvedim), float(tol),
+                                                     ct.byref(rid))
+        if st != ps.SUCCESS:
+            raise ps.PentadError(st, "server submit")
+        self._grids[rid.value] = (desc, grid)
+        return int(rid.value)
+
+    def progress(self, wait: bool = False) -> None:
+        st = self.ps._typed("pentadsolver_server_progress", [self.ct.c_void_p, self.ct.c_int])(
+            self._srv, 1 if wait else 0)
+        if st != self.ps.SUCCESS:
+            raise self.ps.PentadError(st, "server progress")
+
+    def poll(self, capacity: int = 1024) -> list[tuple[int, int]]:
+        ct = self.ct
+        ids = (ct.c_ulonglong * capacity)()
+        bits = (ct.c_int * capacity)()
+        n = ct.c_int(0)
+        st = self.ps._typed("pentadsolver_server_poll",
+                            [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int,
+                             ct.POINTER(ct.c_int)])(self._srv, ids, bits, capacity, ct.byref(n))
+        if st != self.ps.SUCCESS:
+            raise self.ps.PentadError(st, "server poll")
+        out = [(int(ids[i]), int(bits[i])) for i in range(n.value)]
+        for rid, _ in out:
+            self._grids.pop(rid, None)
+        return out
+
+    def stats(self) -> dict:
+        vals = (self.ct.c_size_t * 6)()
+        self.ps._typed("pentadsolver_server_stats",
+                       [self.ct.c_void_p, self.ct.c_void_p, self.ct.c_int])(self._srv, vals, 6)
+        keys = ("queued", "in_flight", "arena_used", "arena_peak", "arena_bytes", "batches")
+        return dict(zip(keys, (int(v) for v in vals)))
+
+    def calibrate(self, grid: dict, reps: int = 3) -> dict:
+        ct, ps = self.ct, self.ps
+        desc = ps._grid_descs([grid])
+        ms = (ct.c_double * 6)()
+        st = ps._typed("pentadsolver_server_calibrate",
+                       [ct.c_void_p, ct.POINTER(ps.GridDesc), ct.c_int, ct.c_void_p])(
+            self._srv, desc, int(reps), ms)
+        if st != ps.SUCCESS:
+            raise ps.PentadError(st, "server calibrate")
+        return {d: {"fp64_ms": round(ms[2 * d], 4), "refined_ms": round(ms[2 * d + 1], 4),
+                    "refine_pays": ms[2 * d + 1] < ms[2 * d]} for d in range(3)}
+
+    def close(self) -> None:
+        if self._srv.value:
+            self.ps._typed("pentadsolver_server_destroy", [self.ct.c_void_p])(self._srv)
+            self._srv = self.ct.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def serve_native(pool: ProblemPool, trace, policy: str, arena_bytes: float, max_batch: int = 64,
+                 refine_steps: int = 1, keep_results: bool = False, calibrate: bool = False,
+                 streams: int = 3):
+    """Replay a trace in real time through the library's serving handle:
+    each request is submitted when its arrival time comes (its iterate a copy
+    of the problem's right-hand side), the handle batches and launches, and
+    completions are polled.  Returns (report, results, status bits, trace)."""
+    import copy
+
+    import torch
+
+    tr = copy.deepcopy(trace)
+    srv = NativeServer(int(arena_bytes), policy, streams=streams, max_batch=max_batch,
+                       refine_steps=refine_steps)
+    cal = None
+    if calibrate and policy == "mixed":
+        big = max(range(len(pool.shapes)), key=pool.points)
+        p = pool.items[big]
+        cal = srv.calibrate({**{k: p[k] for k in ("ds", "dl", "d", "du", "dw")},
+                             "x": p["b"].clone()})
+    pending = sorted(tr, key=lambda r: r.arrival)
+    by_id, xs, bits = {}, {}, {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    i, done = 0, 0
+    while done < len(tr):
+        now = time.perf_counter() - t0
+        while i < len(pending) and pending[i].arrival <= now:
+            r = pending[i]
+            p = pool.items[r.problem]
+            x = p["b"].clone()
+            g = {k: p[k] for k in ("ds", "dl", "d", "du", "dw")}
+            g["x"] = x
+            rid = srv.submit(g, r.solvedim, r.tol)
+            by_id[rid] = r
+            xs[rid] = x
+            r.admitted = r.started = now
+            i += 1
+        srv.progress()
+        for rid, b in srv.poll():
+            r = by_id[rid]
+            r.done = time.perf_counter() - t0
+            bits[r.rid] = b
+            done += 1
+            if not keep_results:
+                xs.pop(rid)
+        if i < len(pending) and srv.stats()["in_flight"] == 0 and not srv.stats()["queued"]:
+            dt = pending[i].arrival - (time.perf_counter() - t0)
+            if dt > 2e-4:
+                time.sleep(dt - 1e-4)
+    torch.cuda.synchronize()
+    rep = report(tr)
+    st = srv.stats()
+    rep.update({"policy": policy, "native": True, "batches": st["batches"],
+                "peak_arena_gb": round(st["arena_peak"] / 1e9, 3)})
+    if cal is not None:
+        rep["calibration"] = cal
+    results = {by_id[rid].rid: x for rid, x in xs.items()} if keep_results else {}
+    srv.close()
+    return rep, results, bits, tr

@@ -113,3 +113,21 @@ def test_mixed_policy_routes_loose_requests_by_measured_cost():
     # without a measurement the loose requests are mixed
     plain = serving.Scheduler(FakeExecutor([1000]), 1e12, policy="mixed")
     assert plain.key_of(loose[1]) == (1, "mixed")
+
+
+def test_native_server_refuses_bad_arguments_before_touching_a_device():
+    import ctypes
+
+    import pentadsolver as ps
+
+    f = ps._typed("pentadsolver_server_create",
+                  [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
+                   ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)])
+    out = ctypes.c_void_p(None)
+    good = dict(arena=1 << 20, nbytes=1 << 20, policy=0, streams=3, batch=8, inflight=3, steps=1)
+    for bad in ({"arena": 0}, {"arena": (1 << 20) + 8}, {"nbytes": 100}, {"policy": 3},
+                {"streams": 0}, {"batch": 0}, {"inflight": 0}, {"steps": 9}):
+        a = {**good, **bad}
+        st = f(None, a["arena"], a["nbytes"], a["policy"], a["streams"], a["batch"],
+               a["inflight"], a["steps"], ctypes.byref(out))
+        assert st == ps.INVALID_VALUE and not out.value, bad
