@@ -18,7 +18,9 @@
            latency and solves/s for the mixed and FP64 policies and for
            sequential plain FP64 calls, at that rate and at saturation; the
            mixed policy first measures, per solve direction, whether the
-           refined form beats plain FP64 and uses it only where it does.
+           refined form beats plain FP64 and uses it only where it does.  Each
+           policy runs twice: the Python loop (serving.serve) and the library's
+           native serving handle (serving.serve_native, pentadsolver_server_*).
 
   odd      odd-size grids: each axis of 255^3 against 256^3, FP64 and FP32, timed as
            single solves (CUDA events, 7 x 930 MB per axis: above L2, no flush),
@@ -367,6 +369,14 @@ def config4(rate=2000.0, seconds=2.0, n_problems=64, budget=150e9, seed=44):
     for policy in ("mixed", "fp64", "sequential"):
         serving.serve(pool, warm, policy, budget)
         torch.cuda.empty_cache()
+    # the native serving handle's arena: the budget less the pool and the
+    # requests' iterates, within what the device has free
+    free, _ = torch.cuda.mem_get_info()
+    arena = int(min(budget - pool.nbytes(), 0.8 * free - pool.nbytes()))
+    out["native_arena_GB"] = round(arena / 1e9, 2)
+    for policy in ("mixed", "fp64", "sequential"):   # warm-up of the native path
+        serving.serve_native(pool, warm, policy, arena)
+        torch.cuda.empty_cache()
     for label, r in (("nominal", rate), ("saturated", math.inf)):
         trace = serving.make_trace(n_req if label == "nominal" else n_req // 2, r, n_problems,
                                    seed=seed + 1)
@@ -376,10 +386,16 @@ def config4(rate=2000.0, seconds=2.0, n_problems=64, budget=150e9, seed=44):
             res[policy] = rep
             del ex
             torch.cuda.empty_cache()
-        res["speedup_mixed_vs_sequential"] = round(res["mixed"]["solves_per_s"] /
-                                                   res["sequential"]["solves_per_s"], 3)
-        res["speedup_fp64_vs_sequential"] = round(res["fp64"]["solves_per_s"] /
-                                                  res["sequential"]["solves_per_s"], 3)
+            rep, _, bits, _ = serving.serve_native(pool, trace, policy, arena, calibrate=True)
+            rep["status_bits_nonzero"] = sum(1 for v in bits.values() if v)
+            res[f"native_{policy}"] = rep
+            torch.cuda.empty_cache()
+        for pre in ("", "native_"):
+            seq = res[f"{pre}sequential"]["solves_per_s"]
+            res[f"{pre}speedup_mixed_vs_sequential"] = round(
+                res[f"{pre}mixed"]["solves_per_s"] / seq, 3)
+            res[f"{pre}speedup_fp64_vs_sequential"] = round(
+                res[f"{pre}fp64"]["solves_per_s"] / seq, 3)
         out[label] = res
     return out
 
