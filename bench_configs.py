@@ -551,11 +551,12 @@ def main():
     ap.add_argument("--n2", type=int, default=512, help="grid edge of config 2")
     ap.add_argument("--grids3", type=int, default=96)
     ap.add_argument("--seconds4", type=float, default=2.0)
+    ap.add_argument("--odd-reps", type=int, default=10, help="timed solves per case (odd)")
     args = ap.parse_args()
     want = {c.strip() for c in args.configs.split(",")}
     runs = {"0": config0, "2": lambda: config2(args.n2), "3": lambda: config3(args.grids3),
             "4": lambda: config4(seconds=args.seconds4), "mesh": config_mesh,
-            "refapp": config_refapp, "odd": config_odd}
+            "refapp": config_refapp, "odd": lambda: config_odd(args.odd_reps)}
     from bench import ClockSampler
 
     for c in ("0", "2", "3", "4", "odd", "mesh", "refapp"):

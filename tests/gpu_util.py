@@ -33,8 +33,8 @@ def direction(ndim: int, solvedim: int) -> int:
 
 def solve_dev(dv: dict, solvedim: int, dims=None, handle=None, buffer=None, stream=None,
               check_status: bool = True):
-    """Solve through the C ABI; by default also require a clean device status
-    word afterwards (no zero pivot, no timed-out wait, no refused launch)."""
+    """Solve through the C ABI; by default also require a clean status word
+    afterwards -- the handle's own (no zero pivot, no timed-out wait)."""
     x = dv["x"]
     dims = ps.dims_of(x) if dims is None else list(dims)
     if buffer is None:
@@ -42,7 +42,7 @@ def solve_dev(dv: dict, solvedim: int, dims=None, handle=None, buffer=None, stre
     ps.gpsv_batch(dv["ds"], dv["dl"], dv["d"], dv["du"], dv["dw"], x, solvedim,
                   buffer=buffer, handle=handle, dims=dims, stream=stream)
     if check_status:
-        st, bits = ps.status_check(stream=stream)
+        st, bits = ps.status_check(stream=stream, handle=handle)
         assert bits == 0, f"device status bits {bits:#x} after solve along {solvedim}"
     return buffer
 

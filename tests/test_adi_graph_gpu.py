@@ -50,9 +50,9 @@ def test_adi_graph_matches_calls_and_oracle(cuda, algo, dims):
         g.replay()
         torch.cuda.synchronize()
         twice = dv["x"].clone()
+        assert ps.status_check(handle=g.handle) == (ps.SUCCESS, 0)   # the graph's handle
     if algo is not None:
         assert fam == [algo] * 3, fam
-    assert ps.status_check()[1] == 0
     ref = co["x"].astype(np.float64)
     for _ in range(2 * iterations):
         for axis in range(3):

@@ -37,6 +37,7 @@ def run_chain(dv, algos, iterations, sync_each: bool, buf):
                     torch.cuda.synchronize()
         torch.cuda.synchronize()
         ran = [h.kernel_that_ran(a) for a in range(3)]
+        assert ps.status_check(handle=h) == (ps.SUCCESS, 0)
     return dv["x"].clone(), ran
 
 

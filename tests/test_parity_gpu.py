@@ -302,7 +302,7 @@ def _run_chain(co, solvedim, dims, env, monkeypatch, offset=None, buffer=True):
     with ps.Handle() as h:
         if not buffer:
             ps.gpsv_batch(*(dv[k] for k in NAMES), solvedim, buffer=None, handle=h)
-            assert ps.status_check()[1] == 0
+            assert ps.status_check(handle=h)[1] == 0
         elif offset is not None:
             eb = dv["x"].element_size()
             need = ps.buffer_size(list(dims), solvedim, eb)

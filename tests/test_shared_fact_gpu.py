@@ -41,19 +41,23 @@ def oracle_solution(co, solvedim):
     return ref["x"]
 
 
-def shared_solve(co, solvedim, dims, buffer="default", check_status=True):
+def shared_solve(co, solvedim, dims, buffer="default", check_status=True, status=None):
+    """Shared-factorisation solve on a handle of its own; with `status` (a
+    list), the handle's (status, bits) are appended to it."""
     dv = to_dev(co)
     dirn = direction(len(dims), solvedim)
     with ps.Handle() as h:
         h.set_algo(dirn, "shared-fact")
         if buffer is None:
             ps.gpsv_batch(*(dv[k] for k in NAMES), solvedim, buffer=None, handle=h)
-            assert ps.status_check()[1] == 0
+            assert ps.status_check(handle=h)[1] == 0
         elif isinstance(buffer, str):
             solve_dev(dv, solvedim, handle=h, check_status=check_status)
         else:
             solve_dev(dv, solvedim, handle=h, buffer=buffer, check_status=check_status)
         fam, var = h.kernel_that_ran(dirn), h.variant_that_ran(dirn)
+        if status is not None:
+            status.append(ps.status_check(handle=h))
     assert fam == "shared-fact", fam
     return dv["x"].cpu().numpy(), var
 
@@ -173,7 +177,7 @@ def test_shared_fact_zero_pivot_is_reported(cuda, dims):
     co["d"][..., 0] = 0.0
     co["dl"][..., 1] = 0.0
     co["ds"][..., 2] = 0.0
-    ps.status_check()
-    shared_solve(co, 0, dims, check_status=False)
-    st, bits = ps.status_check()
+    got = []
+    shared_solve(co, 0, dims, check_status=False, status=got)
+    st, bits = got[0]
     assert st == ps.ZERO_PIVOT and bits & 1
