@@ -387,6 +387,31 @@ def run_ours(args):
     e2e_ms = max_over_ranks(e2e_ms, world, dev)
     e2e_value = whole_job_gbs(alg_bytes_step, e2e_ms, world)
 
+    # ---- one solve per step, end to end: what a single call on host buffers
+    # costs (the copies dominate: 48 B/pt in, 8 B/pt out over PCIe, against
+    # 56 B/pt of HBM traffic for the solve itself); x direction, serialised
+    def single_call_run(reps):
+        S = sets[0]
+        for _ in range(reps):
+            with torch.cuda.stream(stream):
+                for k in ("ds", "dl", "d", "du", "dw", "x"):
+                    S[k].copy_(pinned[k], non_blocking=True)
+                solve_set(0, S)
+                out.copy_(S["x"], non_blocking=True)
+
+    single_call_run(2)
+    torch.cuda.synchronize()
+    c0 = torch.cuda.Event(enable_timing=True)
+    c1 = torch.cuda.Event(enable_timing=True)
+    single_reps = max(3, min(args.steps, 10))
+    c0.record(stream)
+    single_call_run(single_reps)
+    c1.record(stream)
+    torch.cuda.synchronize()
+    single_ms = c0.elapsed_time(c1) / single_reps
+    single_ms = max_over_ranks(single_ms, world, dev)
+    single_value = whole_job_gbs(BYTES_PER_POINT_AXIS * n ** 3, single_ms, world)
+
     # ---- roofline of the dominant kernel -------------------------------------
     # The dominant kernel is the instantiation with the largest share of the
     # timed solves (directions that ran the same variant are one kernel); its
@@ -449,6 +474,11 @@ def run_ours(args):
                 "steps": e2e_steps,
                 "schedule": "pipelined: copies in of step k+1 and out of step k-1 overlap "
                             "the solves of step k (two device sets, two copy streams)"},
+        "e2e_single_call": {"value": round(single_value, 2), "unit": "GB/s",
+                            "ms_per_call": round(single_ms, 3), "h2d_bytes_per_call": h2d,
+                            "d2h_bytes_per_call": d2h, "calls": single_reps,
+                            "note": "one x solve per call: six arrays in from pinned host "
+                                    "memory, solve, result out, serialised on one stream"},
         "graph": {"value": round(whole_job_gbs(alg_bytes_step, graph_ms, world), 2),
                   "unit": "GB/s", "ms_per_step": round(graph_ms, 4),
                   "note": "each step's 150 solves replayed as one CUDA graph (adi.AdiGraph)"},
