@@ -984,7 +984,9 @@ bool shape_ok(const Lines &L, bool contig, int &fmode) {
   const long long cap_both = kTmemCols / tmem_cols_per_stage<F, 0>();
   const long long cap_du = kTmemCols / tmem_cols_per_stage<F, 1>();
   fmode = stages > cap_du ? 2 : stages > cap_both ? 1 : 0;
-  if (L.n * L.n_sys >= (1LL << 31) || tile_count(L, contig) >= (1LL << 31)) return false;
+  // every global offset is formed in 64 bits; line, run and tile indices (and
+  // the TMA coordinates made of them) must stay below 2^31
+  if (L.n_sys >= (1LL << 31) - TS || tile_count(L, contig) >= (1LL << 31)) return false;
   return true;
 }
 
@@ -1236,13 +1238,14 @@ bool tmem_fill_jobs(const SolveArgs<F> *grids, int count, bool contig, int fmode
                     unsigned char *device_base, void *host_jobs, size_t *scratch_offsets,
                     int *total_tiles) {
   TmemJob<F> *J = static_cast<TmemJob<F> *>(host_jobs);
-  int tiles = 0;
+  long long tiles = 0;
   for (int i = 0; i < count; ++i) {
     F *scratch = reinterpret_cast<F *>(device_base + scratch_offsets[i]);
-    if (!fill_job<F>(J[i], grids[i], contig, scratch, tiles)) return false;
+    if (!fill_job<F>(J[i], grids[i], contig, scratch, (int)tiles)) return false;
     tiles += J[i].n_tiles;
+    if (tiles >= (1LL << 31)) return false;  // tile indices of one launch are 32-bit
   }
-  *total_tiles = tiles;
+  *total_tiles = (int)tiles;
   (void)fmode;
   return true;
 }
