@@ -456,6 +456,33 @@ def config_odd(reps=10):
         for pl in plans:
             pl.close()
         os.environ.pop("PENTA_TMEM_LOADS", None)
+    del grids
+    torch.cuda.empty_cache()
+    # aligned 256^3 forced through the bulk-copy layout (against the TMA rows above)
+    with ps.Handle() as h:
+        for dtype in (torch.float64, torch.float32):
+            eb = 8 if dtype == torch.float64 else 4
+            dims = (256, 256, 256)
+            p = dev_problem(dims, 7, dtype)
+            os.environ["PENTA_TMEM_LOADS"] = "bulk"
+            for axis in range(3):
+                buf = ps.alloc_buffer(list(dims), axis, dtype)
+
+                def run():
+                    ps.gpsv_batch(p["ds"], p["dl"], p["d"], p["du"], p["dw"], p["x"], axis,
+                                  buffer=buf, handle=h)
+
+                ms = timed(run, reps=reps, warmup=2)
+                d = 0 if axis == 0 else (2 if axis == 2 else 1)
+                gbs = 7 * eb * 256 ** 3 / (ms * 1e-3) / 1e9
+                out["rows"].append({"dtype": "f64" if eb == 8 else "f32", "edge": 256,
+                                    "axis": axis, "loads": "bulk",
+                                    "variant": h.variant_that_ran(d), "us": round(ms * 1e3, 1),
+                                    "GBps": round(gbs, 1), "frac": round(gbs / pk, 3)})
+                del buf
+            os.environ.pop("PENTA_TMEM_LOADS", None)
+            del p
+            torch.cuda.empty_cache()
     out["peak_GBps"] = pk
     return out
 
