@@ -615,10 +615,12 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
           err = launch_tmem<F>(a, mc, ctx.sm_count, stream);
           if (err == cudaSuccess) {
             char vb[96];
+            const char *ld = "";
+            if (mc.loads == 1) ld = tmem_groups<F>(a, contig) > 0 ? " grp" : " bulk";
             std::snprintf(vb, sizeof vb, "thomas-pcr:tmem P2 S16 R%d x%d/%d%s%s%s", mc.R,
                           mc.stages, mc.xstages,
-                          mc.fmode == 2 ? " fbuf" : mc.fmode == 1 ? " w2s" : "",
-                          mc.loads == 1 ? " bulk" : "", contig ? " contig" : "");
+                          mc.fmode == 2 ? " fbuf" : mc.fmode == 1 ? " w2s" : "", ld,
+                          contig ? " contig" : "");
             record(ctx, dir, "thomas-pcr", vb);
             return PENTAD_STATUS_SUCCESS;
           }
@@ -884,7 +886,7 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
         ++last;
       int tiles = 0;
       if (!tmem_fill_jobs<F>(args.data() + first, (int)(last - first), contig,
-                             (int)gw2s[order[first]], base,
+                             (int)gw2s[order[first]], (int)gloads[order[first]], base,
                              static_cast<unsigned char *>(host) + first * jb,
                              job_offs.data() + first, &tiles)) {
         std::free(host);
@@ -937,7 +939,7 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
   int n_bulk = 0;
   for (int i : order) n_bulk += gloads[i] ? 1 : 0;
   std::snprintf(d, sizeof d,
-                "tmem-batch %s grids=%d tiles=%d launches=%d%s ctas=%d alone=%d bulk=%d",
+                "tmem-batch %s grids=%d tiles=%d launches=%d%s ctas=%d alone=%d pitched=%d",
                 sizeof(F) == 8 ? "f64" : "f32", p->n_jobs, total_tiles, (int)groups.size(),
                 w2s ? " w2s" : "", p->ctas, (int)singles.size(), n_bulk);
   p->desc = d;

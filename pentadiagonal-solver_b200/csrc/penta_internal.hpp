@@ -97,7 +97,7 @@ struct TmemConfig {
   int xstages;   // read-back stages per consumer warp
   int R;         // rows per stage
   size_t smem;   // dynamic shared memory per CTA
-  int loads;     // 0: TMA tiles / element copies; 1: bulk copies (misaligned rows or runs)
+  int loads;     // 0: TMA tiles / element copies; 1: pitched (group-view TMA, bulk copies)
 };
 template <typename F> const std::vector<TmemConfig> &tmem_configs();
 template <typename F> int tmem_occupancy(const TmemConfig &c);
@@ -106,8 +106,10 @@ template <typename F> bool tmem_shape(const Lines &L, bool contig, int &fmode);
 template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig, int fmode);
 template <typename F>
 bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf, int &fmode);
-// The stage layout (TmemConfig::loads) a grid's loads take.
+// The stage layout (TmemConfig::loads) a grid's loads take, and for the
+// pitched layout the group size of its TMA view (0: bulk copies only).
 template <typename F> int tmem_loads(const SolveArgs<F> &a, bool contig);
+template <typename F> int tmem_groups(const SolveArgs<F> &a, bool contig);
 template <typename F>
 cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count,
                         cudaStream_t stream);
@@ -116,7 +118,7 @@ cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count
 // device_base + scratch_offsets[i] (128-byte aligned for L2 discards).
 template <typename F> size_t tmem_job_bytes();
 template <typename F>
-bool tmem_fill_jobs(const SolveArgs<F> *grids, int count, bool contig, int fmode,
+bool tmem_fill_jobs(const SolveArgs<F> *grids, int count, bool contig, int fmode, int loads,
                     unsigned char *device_base, void *host_jobs, size_t *scratch_offsets,
                     int *total_tiles);
 template <typename F>

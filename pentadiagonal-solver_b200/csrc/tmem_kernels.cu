@@ -95,6 +95,10 @@ template <typename F> struct alignas(64) TmemJob {
   int n, mt, inner, tpr, n_sys, n_tiles, tile_base;
   int tma;              // 1: TMA tiles; 0: element copies (misaligned grid)
   int bulk;             // 1: every array 16-byte aligned (bulk-copy loads possible)
+  int grp;              // pitched layout: maps[0..5] view groups of grp rows (strided)
+                        // or lines (x) so that each group is 16-byte periodic; 0: none
+  int tail;             // first tile (x) / the run (strided) whose rows or lines lie
+                        // outside whole groups: fetched by bulk copies
 };
 
 namespace {
@@ -232,7 +236,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   struct Geo {
     const TmemJob<F> *J;
     F *x, *scratch;
-    int n, mt, inner, tpr, n_sys, tile_base, n_tiles, tma;
+    int n, mt, inner, tpr, n_sys, tile_base, n_tiles, tma, grp, tail;
   };
   auto load_geo = [&](const TmemJob<F> *J, Geo &g) {
     g.J = J;
@@ -246,6 +250,8 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
     g.tile_base = J->tile_base;
     g.n_tiles = J->n_tiles;
     g.tma = J->tma;
+    g.grp = J->grp;
+    g.tail = J->tail;
   };
   auto tile_coords = [&](const Geo &g, int tile, int &c0, int &c2) {
     if (CONTIG) {
@@ -281,14 +287,15 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
           for (int q = 0; q < 6; ++q) arrs[q] = J->arr[q];
       }
       const bool tma = LD == 0 && JG.tma != 0;
+      const bool maps_used = tma || (LD == 1 && J->grp > 0);
       if (BATCH && cursor != fenced) {  // a new grid: its maps, and the next grid's
         if (lane == 0) {
-          if (tma)
+          if (maps_used)
             for (int q = 0; q < 6; ++q) {
               tensormap_acquire(&J->maps[q]);  // host-written: acquire once
               tensormap_prefetch(&J->maps[q]);
             }
-          if (cursor + 1 < n_jobs && jobs[cursor + 1].tma)
+          if (cursor + 1 < n_jobs && (jobs[cursor + 1].tma || jobs[cursor + 1].grp))
             for (int q = 0; q < 6; ++q) tensormap_prefetch(&jobs[cursor + 1].maps[q]);
         }
         fenced = cursor;
@@ -312,7 +319,45 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         const int r_up = g * R;
         const int r_dn = 2 * mt - (g + 1) * R;  // lower half, virtual rows included
         F *dst = ring + slot * SE;
-        if constexpr (LD == 1) {
+        bool by_groups = false;
+        if constexpr (LD == 1)
+          by_groups = JG.grp > 0 && (CONTIG ? (c0 / TS < JG.tail) : (c2 != JG.tail));
+        if (LD == 1 && by_groups) {
+          // One TMA box per residue class of the group view: along x the
+          // lines c0 + k grp + sub (box {R + chunk, 16 / grp} at the aligned-
+          // down first row), strided the rows whose global index G = c2 n + r
+          // has G % grp == sub (box {16 + chunk, R / grp} of consecutive
+          // groups).  Class sub lands at sub (16/grp) PL (x) or sub (R/grp) PS
+          // (strided) in its tile; the forward warp reads it there.
+          if (lane == 0) {
+            const bool lower = r_dn < n;  // else all rows are virtual: not loaded
+            const int gq = JG.grp, lgq = gq == 4 ? 2 : (gq == 2 ? 1 : 3);
+            mbar_arrive_n(&full[slot], 31);
+            mbar_expect_tx(&full[slot], (lower ? 12u : 6u) * (unsigned)(BOXL * sizeof(F)));
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                if (h && !lower) continue;
+                const CUtensorMap *map = &J->maps[h ? kMirror[q] : q];
+                F *const tb = dst + (2 * q + h) * BOXL;
+                const int r0 = h ? r_dn : r_up;
+                for (int sub = 0; sub < gq; ++sub) {
+                  if (CONTIG) {
+                    const int sh = (sub * (n & (G::EPC - 1))) & (G::EPC - 1);
+                    tma_load_2d_hint(tb + sub * (TS >> lgq) * PL, map, &full[slot],
+                                     sub * n + r0 - sh, c0 >> lgq, pol_in);
+                  } else {
+                    const long long G0 = (long long)c2 * n + r0;
+                    const int rr0 = (sub - (int)(G0 & (gq - 1))) & (gq - 1);
+                    const int sh = (sub * (inner & (G::EPC - 1))) & (G::EPC - 1);
+                    tma_load_2d_hint(tb + sub * (R >> lgq) * PS, map, &full[slot],
+                                     sub * inner + c0 - sh, (int)((G0 + rr0) >> lgq), pol_in);
+                  }
+                }
+              }
+          }
+        } else if constexpr (LD == 1) {
           // Bulk copies of 16-byte aligned supersets.  Copy k of the stage:
           // tile bx = 2 q + half, then line (along x) or row (strided) `sub`.
           // Each lane arrives once with its own byte count, then issues its
@@ -504,7 +549,30 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
       // chunk is the shift.  Stages start at multiples of R rows (R a multiple
       // of the chunk), so a tile's shifts repeat from stage to stage.
       int ldm[LD == 1 ? R : 1];
-      if constexpr (LD == 1) {
+      bool by_groups = false;
+      if constexpr (LD == 1)
+        by_groups = JG.grp > 0 && (CONTIG ? (c0 / TS < JG.tail) : (c2 != JG.tail));
+      if (LD == 1 && by_groups) {
+        // the group view's classes (see the feeding warp)
+        const int gq = JG.grp, lgq = gq == 4 ? 2 : (gq == 2 ? 1 : 3);
+        if constexpr (CONTIG) {
+          const int sub = sys & (gq - 1), k = sys >> lgq;
+          const int sh = (sub * (n & (G::EPC - 1))) & (G::EPC - 1);
+          const int b = part * BOXL + sub * (TS >> lgq) * PL + k * PL + sh;
+#pragma unroll
+          for (int r = 0; r < R; ++r) ldm[r] = b + (part ? (R - 1 - r) : r);
+        } else {
+          const int q0 = (int)(((long long)c2 * n) & (gq - 1));
+          const int im = JG.inner & (G::EPC - 1);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int rr = part ? (R - 1 - r) : r;
+            const int sub = (q0 + rr) & (gq - 1);
+            ldm[r] = part * BOXL + sub * (R >> lgq) * PS + (rr >> lgq) * PS +
+                     ((sub * im) & (G::EPC - 1)) + sys;
+          }
+        }
+      } else if constexpr (LD == 1) {
         if constexpr (CONTIG) {
           const int sh = (int)(((long long)(c0 + sys) * n) & (G::EPC - 1));
 #pragma unroll
@@ -1014,8 +1082,46 @@ template <typename F> size_t job_scratch_bytes(const Lines &L, bool contig, int 
          (fmode == 2 ? 3 : fmode == 1 ? 2 : 1) * sizeof(F);
 }
 
+// The group view of a grid whose rows (x) or runs (strided) are not 16-byte
+// aligned: `grp` consecutive lines (x) or rows (strided) form a 16-byte
+// periodic group, so maps over {grp * stride, groups} are valid tensor maps.
+// Returns grp, or 0 when the view does not apply (or bulk copies are forced).
+template <typename F> int group_size(const SolveArgs<F> &a, bool contig) {
+  const char *e = std::getenv("PENTA_TMEM_LOADS");
+  if (e != nullptr && !std::strcmp(e, "bulk")) return 0;
+  if (!bulk_ok<F>(a) || tma_ok<F>(a, contig) || tensor_map_encoder() == nullptr) return 0;
+  const long long m = contig ? a.L.n : a.L.inner;
+  const long long bytes = m * (long long)sizeof(F);
+  const int g = bytes % 16 == 0 ? 1 : (bytes % 8 == 0 ? 2 : (bytes % 4 == 0 ? 4 : 8));
+  if (g > 4 || g * m >= (1LL << 31)) return 0;
+  const long long groups = contig ? a.L.n_sys / g : a.L.n * (a.L.n_sys / a.L.inner) / g;
+  if (groups < 1 || groups >= (1LL << 31)) return 0;
+  return g;
+}
+
 template <typename F>
-bool fill_job(TmemJob<F> &J, const SolveArgs<F> &a, bool contig, F *scratch, int tile_base) {
+bool encode_groups(CUtensorMap *m, const F *ptr, const Lines &L, bool contig, int g, int R) {
+  auto fn = tensor_map_encoder();
+  if (fn == nullptr) return false;
+  constexpr int EPC = 16 / (int)sizeof(F);
+  const CUtensorMapDataType dt =
+      sizeof(F) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const long long stride = contig ? L.n : L.inner;
+  const long long groups = contig ? L.n_sys / g : L.n * (L.n_sys / L.inner) / g;
+  const cuuint64_t dims[2] = {(cuuint64_t)(g * stride), (cuuint64_t)groups};
+  const cuuint64_t strides[1] = {(cuuint64_t)(g * stride) * sizeof(F)};
+  const cuuint32_t box[2] = {(cuuint32_t)(contig ? R + EPC : TS + EPC),
+                             (cuuint32_t)(contig ? TS / g : R / g)};
+  const cuuint32_t es[2] = {1, 1};
+  return fn(m, dt, 2, const_cast<F *>(ptr), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            contig ? CU_TENSOR_MAP_L2_PROMOTION_L2_256B : CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename F>
+bool fill_job(TmemJob<F> &J, const SolveArgs<F> &a, bool contig, F *scratch, int tile_base,
+              int loads = 0) {
   std::memset(&J, 0, sizeof(J));
   const int R = contig ? tmem_rows_per_stage<F, true>() : tmem_rows_per_stage<F, false>();
   const F *ptrs[6] = {a.ds, a.dl, a.d, a.du, a.dw, a.x};
@@ -1026,6 +1132,22 @@ bool fill_job(TmemJob<F> &J, const SolveArgs<F> &a, bool contig, F *scratch, int
     if (J.tma && !encode<F>(&J.maps[q], ptrs[q], a.L, contig, R)) J.tma = 0;
   }
   if (J.tma && contig && !encode<F>(&J.maps[6], a.x, a.L, contig, R, true)) J.tma = 0;
+  J.grp = 0;
+  J.tail = contig ? 0x7fffffff : -1;
+  if (loads == 1) {  // pitched layout: the group view where it applies
+    const int g = group_size<F>(a, contig);
+    bool ok = g > 0;
+    for (int q = 0; ok && q < 6; ++q) ok = encode_groups<F>(&J.maps[q], ptrs[q], a.L, contig, g, R);
+    if (ok) {
+      J.grp = g;
+      if (contig) {
+        if (a.L.n_sys % g != 0) J.tail = (int)(a.L.n_sys / g * g / TS);
+      } else {
+        const long long outer = a.L.n_sys / a.L.inner;
+        if ((a.L.n * outer) % g != 0) J.tail = (int)(outer - 1);
+      }
+    }
+  }
   J.x = a.x;
   J.scratch = scratch;
   J.n = (int)a.L.n;
@@ -1157,18 +1279,23 @@ template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig, int
   return job_scratch_bytes<F>(L, contig, fmode);
 }
 
-// Which stage layout a grid's loads use: 0 for TMA tiles (aligned grids) or
-// element copies (arrays not 16-byte aligned), 1 for bulk copies (arrays
-// 16-byte aligned, rows or runs not).  PENTA_TMEM_LOADS=bulk also sends
-// aligned grids through bulk copies, =element keeps misaligned grids on
-// element copies (both for measurements and tests).
+// Which stage layout a grid's loads use.  0: TMA tiles (aligned rows or
+// runs) or element copies (PENTA_TMEM_LOADS=element, or arrays not 16-byte
+// aligned).  1: the pitched layout -- for misaligned rows or runs, TMA boxes
+// of the group view (group_size), with the rows or lines outside whole groups
+// fetched by bulk copies of aligned supersets; PENTA_TMEM_LOADS=bulk fetches
+// every tile by bulk copies (for measurement: each cp.async.bulk is a TMA
+// request of 80-144 bytes, and B200's TMA unit takes about one request per 18
+// cycles per SM, 1.2-2.4 TB/s in all).
 template <typename F> int tmem_loads(const SolveArgs<F> &a, bool contig) {
   const char *e = std::getenv("PENTA_TMEM_LOADS");
-  const bool force_bulk = e != nullptr && !std::strcmp(e, "bulk");
-  const bool no_bulk = e != nullptr && !std::strcmp(e, "element");
-  if (no_bulk || !bulk_ok<F>(a)) return 0;
-  if (force_bulk) return 1;
-  return tma_ok<F>(a, contig) ? 0 : 1;
+  if (e != nullptr && !std::strcmp(e, "element")) return 0;
+  if (e != nullptr && !std::strcmp(e, "bulk")) return bulk_ok<F>(a) ? 1 : 0;
+  return group_size<F>(a, contig) > 0 ? 1 : 0;
+}
+
+template <typename F> int tmem_groups(const SolveArgs<F> &a, bool contig) {
+  return tmem_loads<F>(a, contig) == 1 ? group_size<F>(a, contig) : 0;
 }
 
 template <typename F>
@@ -1210,7 +1337,7 @@ template <typename F>
 cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count,
                         cudaStream_t stream) {
   TmemJob<F> J;
-  if (!fill_job<F>(J, a, c.contig, static_cast<F *>(a.scratch), 0))
+  if (!fill_job<F>(J, a, c.contig, static_cast<F *>(a.scratch), 0, c.loads))
     return cudaErrorInvalidValue;
   if (c.loads == 1 && !J.bulk) return cudaErrorInvalidValue;  // bulk loads need aligned arrays
   int flags = ((reinterpret_cast<uintptr_t>(a.scratch) % 128 == 0) ? 1 : 0);
@@ -1234,14 +1361,14 @@ cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count
 template <typename F> size_t tmem_job_bytes() { return sizeof(TmemJob<F>); }
 
 template <typename F>
-bool tmem_fill_jobs(const SolveArgs<F> *grids, int count, bool contig, int fmode,
+bool tmem_fill_jobs(const SolveArgs<F> *grids, int count, bool contig, int fmode, int loads,
                     unsigned char *device_base, void *host_jobs, size_t *scratch_offsets,
                     int *total_tiles) {
   TmemJob<F> *J = static_cast<TmemJob<F> *>(host_jobs);
   long long tiles = 0;
   for (int i = 0; i < count; ++i) {
     F *scratch = reinterpret_cast<F *>(device_base + scratch_offsets[i]);
-    if (!fill_job<F>(J[i], grids[i], contig, scratch, (int)tiles)) return false;
+    if (!fill_job<F>(J[i], grids[i], contig, scratch, (int)tiles, loads)) return false;
     tiles += J[i].n_tiles;
     if (tiles >= (1LL << 31)) return false;  // tile indices of one launch are 32-bit
   }
@@ -1293,10 +1420,12 @@ template cudaError_t launch_tmem<float>(const SolveArgs<float> &, const TmemConf
                                         cudaStream_t);
 template size_t tmem_job_bytes<double>();
 template size_t tmem_job_bytes<float>();
-template bool tmem_fill_jobs<double>(const SolveArgs<double> *, int, bool, int, unsigned char *,
-                                     void *, size_t *, int *);
-template bool tmem_fill_jobs<float>(const SolveArgs<float> *, int, bool, int, unsigned char *,
-                                    void *, size_t *, int *);
+template bool tmem_fill_jobs<double>(const SolveArgs<double> *, int, bool, int, int,
+                                     unsigned char *, void *, size_t *, int *);
+template bool tmem_fill_jobs<float>(const SolveArgs<float> *, int, bool, int, int,
+                                    unsigned char *, void *, size_t *, int *);
+template int tmem_groups<double>(const SolveArgs<double> &, bool);
+template int tmem_groups<float>(const SolveArgs<float> &, bool);
 template cudaError_t launch_tmem_batch<double>(const void *, int, int, bool, int, int, bool,
                                                int, int *, cudaStream_t);
 template cudaError_t launch_tmem_batch<float>(const void *, int, int, bool, int, int, bool, int,

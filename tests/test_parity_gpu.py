@@ -404,11 +404,13 @@ def _loads_run(co, solvedim, loads, monkeypatch):
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 def test_misaligned_grids_bulk_element_and_tma_loads_agree(cuda, dims, dtype, monkeypatch):
     """Rows (x) or runs (y, z) that do not start on 16-byte boundaries: the
-    Tensor-Memory kernel fetches them by bulk copies of aligned supersets
-    (default), or by element copies (PENTA_TMEM_LOADS=element); aligned
-    rows and runs by TMA tiles, or by bulk copies when forced.  The same
-    arithmetic runs on the same values whichever way they arrive, so the
-    results are identical bit for bit, and equal the oracle's."""
+    Tensor-Memory kernel fetches them as TMA boxes of a group view (default:
+    pairs or quadruples of rows / lines are 16-byte periodic; the ones
+    outside whole groups by bulk copies), by element copies
+    (PENTA_TMEM_LOADS=element), or all by bulk copies of aligned supersets
+    (=bulk); aligned rows and runs by TMA tiles.  The same arithmetic runs on
+    the same values whichever way they arrive, so the results are identical
+    bit for bit, and equal the oracle's."""
     eb = np.dtype(dtype).itemsize
     co = fixtures.random_dominant(dims, 91, dtype)
     for solvedim in range(3):
@@ -423,8 +425,9 @@ def test_misaligned_grids_bulk_element_and_tma_loads_agree(cuda, dims, dtype, mo
         x_elem, v_elem = _loads_run(co, solvedim, "element", monkeypatch)
         x_bulk, v_bulk = _loads_run(co, solvedim, "bulk", monkeypatch)
         assert "tmem" in v_auto and "tmem" in v_elem and "tmem" in v_bulk
-        assert ("bulk" in v_auto) == (not aligned), (dims, solvedim, v_auto)
-        assert "bulk" not in v_elem and "bulk" in v_bulk, (v_elem, v_bulk)
+        assert ("grp" in v_auto) == (not aligned), (dims, solvedim, v_auto)
+        assert "grp" not in v_elem and "bulk" not in v_elem, v_elem
+        assert "bulk" in v_bulk, v_bulk
         assert fwd_err(x_auto, ref) <= FWD_TOL[dtype], (dims, solvedim, v_auto)
         assert np.array_equal(x_auto.view(np.uint8), x_elem.view(np.uint8)), (dims, solvedim)
         assert np.array_equal(x_auto.view(np.uint8), x_bulk.view(np.uint8)), (dims, solvedim)
