@@ -217,6 +217,26 @@ EXTERN_C PENTAD_API pentadStatus_t pentadsolver_autotune_solve(
     int t_ndim, int t_solvedim, void *t_buffer, size_t t_buffer_bytes, int reps, void *stream,
     char *report, size_t report_len);
 
+/* ---- ADI iterations as one CUDA graph --------------------------------------
+ * The loop of the reference's ADI application (apps/adi_cuda.cu:167-176: one
+ * pentadsolver_gpsv_batch call per direction and step) captured once:
+ * `iterations` steps of x, then y, then z solves of one grid in place (through
+ * pentadsolver_{D,S}_gpsv_batch_ex with `handle`, so its algorithm choices --
+ * shared factorisation with its table cached across steps, for instance --
+ * hold), replayed with one call.  `t_buffer` is the x direction's
+ * reference-sized buffer (pentadsolver_buffer_size_ex with solvedim 0); an
+ * eager warm-up before capture solves a copy of x kept in its unused tail, so
+ * x is untouched until the first replay and nothing is allocated.  The
+ * arrays and the buffer must stay valid while the graph lives. */
+typedef struct pentadsolver_adi_s *pentadsolver_adi_t;
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_adi_create(
+    pentadsolver_handle_t handle, int elem_bytes, const void *ds, const void *dl, const void *d,
+    const void *du, const void *dw, void *x, const int *t_dims, int t_ndim, int iterations,
+    void *t_buffer, size_t t_buffer_bytes, pentadsolver_adi_t *adi);
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_adi_replay(pentadsolver_adi_t adi, void *stream);
+EXTERN_C PENTAD_API int pentadsolver_adi_launches(pentadsolver_adi_t adi);
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_adi_destroy(pentadsolver_adi_t adi);
+
 /* ---- Serving handle: a continuous-batching request loop -------------------
  * No counterpart in the reference.  Requests -- one FP64 grid (the caller's
  * device arrays; x is the right-hand side in and the solution out) and a
