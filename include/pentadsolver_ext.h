@@ -226,8 +226,9 @@ EXTERN_C PENTAD_API pentadStatus_t pentadsolver_autotune_solve(
  * hold), replayed with one call.  `t_buffer` is the x direction's
  * reference-sized buffer (pentadsolver_buffer_size_ex with solvedim 0); an
  * eager warm-up before capture solves a copy of x kept in its unused tail, so
- * x is untouched until the first replay and nothing is allocated.  The
- * arrays and the buffer must stay valid while the graph lives. */
+ * x is untouched until the first replay and nothing is allocated.  Creation
+ * synchronises the device.  The arrays and the buffer must stay valid while
+ * the graph lives. */
 typedef struct pentadsolver_adi_s *pentadsolver_adi_t;
 EXTERN_C PENTAD_API pentadStatus_t pentadsolver_adi_create(
     pentadsolver_handle_t handle, int elem_bytes, const void *ds, const void *dl, const void *d,

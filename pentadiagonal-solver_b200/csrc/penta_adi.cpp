@@ -73,6 +73,12 @@ extern "C" PENTAD_API pentadStatus_t pentadsolver_adi_create(
   unsigned char *copy = reinterpret_cast<unsigned char *>((end - xbytes) & ~uintptr_t(255));
   const size_t scratch_bytes = (size_t)(copy - base);
   const void *arrays[5] = {ds, dl, d, du, dw};
+  // work queued on any stream may still use the buffer or write x: creation
+  // waits for the device first (creation is set-up, not the solve path)
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    cudaGetLastError();
+    return PENTAD_STATUS_EXECUTION_FAILED;
+  }
   cudaStream_t s = nullptr;
   if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();

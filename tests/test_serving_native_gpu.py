@@ -97,8 +97,8 @@ def test_native_server_respects_a_small_arena(cuda):
 
 
 def test_native_server_rejects_a_request_larger_than_its_arena(cuda):
-    pool = _pool(seed=51, count=2, cap=300_000)
-    srv = serving.NativeServer(1 << 20, "fp64")   # 1 MiB: no grid's plan fits
+    pool = serving.ProblemPool([(128, 128, 64)], seed=51)   # plan scratch of several MB
+    srv = serving.NativeServer(1 << 20, "fp64")   # 1 MiB: the grid's plan cannot fit
     p = pool.items[0]
     rid = srv.submit({**{k: p[k] for k in ("ds", "dl", "d", "du", "dw")}, "x": p["b"].clone()},
                      0, 1e-13)
