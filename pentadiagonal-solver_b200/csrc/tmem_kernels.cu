@@ -129,7 +129,23 @@ template <typename F, bool CONTIG, int FM, int ST, int XST, int LD> struct TmemG
   // + one chunk (along x)
   static constexpr int PS = TS + EPC;
   static constexpr int PL = R + EPC;
-  static constexpr int BOXL = LD == 0 ? BOX : (CONTIG ? TS * PL : R * PS);  // per tile
+  // The group view's residue classes each land in a block of rows/grp rows
+  // (strided, pitch PS) or 16/grp lines (x, pitch PL), and a TMA destination
+  // must start on a 128-byte boundary: CPg = one class block of group size g,
+  // rounded up to 128 bytes.  A tile holds g of them, or the bulk layout.
+  static constexpr int kRows = CONTIG ? TS : R;
+  static constexpr int kPitch = CONTIG ? PL : PS;
+  static constexpr int cls(int g) {
+    return ((kRows / g) * kPitch * (int)sizeof(F) + 127) / 128 * 128 / (int)sizeof(F);
+  }
+  static constexpr int CP2 = cls(2), CP4 = cls(4);
+  static constexpr int kPitched0 = kRows * kPitch;
+  static constexpr int kPitched1 = 2 * CP2 > kPitched0 ? 2 * CP2 : kPitched0;
+  static constexpr int kPitched =
+      (sizeof(F) == 4 && 4 * CP4 > kPitched1) ? 4 * CP4 : kPitched1;  // FP32 groups of 4
+  static constexpr int kUnit = 128 / (int)sizeof(F);
+  static constexpr int BOXL =
+      LD == 0 ? BOX : (kPitched + kUnit - 1) / kUnit * kUnit;  // per tile, 128 B multiple
   static constexpr int SE = 12 * BOXL;                // forward stage
   static constexpr int XE = 2 * R * TS * PW;          // read-back stage
   static constexpr int OBE = CONTIG ? 8 * BOX : 0;    // output: 2 buffers x 2 halves x 2R rows
@@ -144,8 +160,10 @@ template <typename F, bool CONTIG, int FM, int ST, int XST, int LD> struct TmemG
   // at least 116 KB, so that one CTA holds an SM (and all of its TMEM)
   static constexpr size_t kSmem = kUsed > 118784 ? kUsed : 118784;
   static_assert(kSmem <= 232448, "shared memory per CTA");
-  static_assert((BOXL * sizeof(F)) % 16 == 0 && (PS * sizeof(F)) % 16 == 0 &&
-                    (PL * sizeof(F)) % 16 == 0,
+  static_assert((BOXL * sizeof(F)) % 128 == 0 && (CP2 * sizeof(F)) % 128 == 0 &&
+                    (CP4 * sizeof(F)) % 128 == 0,
+                "TMA destinations must stay 128-byte aligned");
+  static_assert((PS * sizeof(F)) % 16 == 0 && (PL * sizeof(F)) % 16 == 0,
                 "bulk-copy destinations must stay 16-byte aligned");
   static_assert(R * (FM == 0 ? 2 : 1) * (int)sizeof(F) / 4 == kCols, "TMEM columns per stage");
 };
@@ -173,7 +191,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   using G = TmemGeom<F, CONTIG, FM, ST, XST, LD>;
   using V2 = typename Vec2<F>::T;
   constexpr int R = G::R, BOX = G::BOX, SE = G::SE, XE = G::XE, PW = G::PW, NB = G::NB;
-  constexpr int BOXL = G::BOXL, PS = G::PS, PL = G::PL;
+  constexpr int BOXL = G::BOXL, PS = G::PS, PL = G::PL, CP2 = G::CP2, CP4 = G::CP4;
   constexpr int EPC = 16 / (int)sizeof(F);  // elements per 16-byte chunk
   constexpr int CW = (int)sizeof(F) / 4;    // TMEM columns per value
   constexpr int kMirror[6] = {4, 3, 2, 1, 0, 5};
@@ -332,8 +350,11 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
           if (lane == 0) {
             const bool lower = r_dn < n;  // else all rows are virtual: not loaded
             const int gq = JG.grp, lgq = gq == 4 ? 2 : (gq == 2 ? 1 : 3);
+            const int cpe = gq == 4 ? CP4 : CP2;  // class block (128-byte multiple)
             mbar_arrive_n(&full[slot], 31);
-            mbar_expect_tx(&full[slot], (lower ? 12u : 6u) * (unsigned)(BOXL * sizeof(F)));
+            // each box is rows/grp x pitch elements; grp of them per tile half
+            constexpr unsigned kTileBytes = (unsigned)(G::kRows * G::kPitch * sizeof(F));
+            mbar_expect_tx(&full[slot], (lower ? 12u : 6u) * kTileBytes);
 #pragma unroll
             for (int q = 0; q < 6; ++q)
 #pragma unroll
@@ -345,13 +366,13 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
                 for (int sub = 0; sub < gq; ++sub) {
                   if (CONTIG) {
                     const int sh = (sub * (n & (G::EPC - 1))) & (G::EPC - 1);
-                    tma_load_2d_hint(tb + sub * (TS >> lgq) * PL, map, &full[slot],
+                    tma_load_2d_hint(tb + sub * cpe, map, &full[slot],
                                      sub * n + r0 - sh, c0 >> lgq, pol_in);
                   } else {
                     const long long G0 = (long long)c2 * n + r0;
                     const int rr0 = (sub - (int)(G0 & (gq - 1))) & (gq - 1);
                     const int sh = (sub * (inner & (G::EPC - 1))) & (G::EPC - 1);
-                    tma_load_2d_hint(tb + sub * (R >> lgq) * PS, map, &full[slot],
+                    tma_load_2d_hint(tb + sub * cpe, map, &full[slot],
                                      sub * inner + c0 - sh, (int)((G0 + rr0) >> lgq), pol_in);
                   }
                 }
@@ -555,10 +576,11 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
       if (LD == 1 && by_groups) {
         // the group view's classes (see the feeding warp)
         const int gq = JG.grp, lgq = gq == 4 ? 2 : (gq == 2 ? 1 : 3);
+        const int cpe = gq == 4 ? CP4 : CP2;
         if constexpr (CONTIG) {
           const int sub = sys & (gq - 1), k = sys >> lgq;
           const int sh = (sub * (n & (G::EPC - 1))) & (G::EPC - 1);
-          const int b = part * BOXL + sub * (TS >> lgq) * PL + k * PL + sh;
+          const int b = part * BOXL + sub * cpe + k * PL + sh;
 #pragma unroll
           for (int r = 0; r < R; ++r) ldm[r] = b + (part ? (R - 1 - r) : r);
         } else {
@@ -568,8 +590,8 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
           for (int r = 0; r < R; ++r) {
             const int rr = part ? (R - 1 - r) : r;
             const int sub = (q0 + rr) & (gq - 1);
-            ldm[r] = part * BOXL + sub * (R >> lgq) * PS + (rr >> lgq) * PS +
-                     ((sub * im) & (G::EPC - 1)) + sys;
+            ldm[r] = part * BOXL + sub * cpe + (rr >> lgq) * PS + ((sub * im) & (G::EPC - 1)) +
+                     sys;
           }
         }
       } else if constexpr (LD == 1) {
@@ -1235,16 +1257,16 @@ template <typename F, bool CONTIG, int FM, int ST, int XST, int LD> int tmem_occ
   X(float, true, 2, 2, 2, 0)    \
   X(float, false, 2, 3, 2, 0)   \
   X(double, true, 0, 2, 4, 1)   \
-  X(double, false, 0, 3, 4, 1)  \
+  X(double, false, 0, 3, 3, 1)  \
   X(double, true, 1, 2, 3, 1)   \
   X(double, false, 1, 2, 4, 1)  \
   X(double, true, 2, 2, 2, 1)   \
   X(double, false, 2, 2, 2, 1)  \
   X(float, true, 0, 2, 4, 1)    \
-  X(float, false, 0, 3, 4, 1)   \
-  X(float, true, 1, 2, 3, 1)    \
+  X(float, false, 0, 2, 4, 1)   \
+  X(float, true, 1, 2, 2, 1)    \
   X(float, false, 1, 2, 4, 1)   \
-  X(float, true, 2, 2, 2, 1)    \
+  X(float, true, 2, 2, 1, 1)    \
   X(float, false, 2, 2, 2, 1)
 
 template <typename F> const std::vector<TmemConfig> &tmem_configs() {
