@@ -416,7 +416,7 @@ def config_odd(reps=10):
                 dims = (edge, edge, edge)
                 p = dev_problem(dims, 7, dtype)
                 b = p["x"].clone()
-                for loads in ("", "element"):
+                for loads in ("", "group"):
                     if loads and edge % (16 // eb) == 0:
                         continue   # aligned: TMA tiles either way
                     os.environ["PENTA_TMEM_LOADS"] = loads
@@ -446,7 +446,7 @@ def config_odd(reps=10):
     sub = sorted(dims_list, key=math.prod)[:16]
     grids = [dev_problem(d, 500 + i) for i, d in enumerate(sub)]
     pts = sum(math.prod(d) for d in sub)
-    for loads in ("", "element"):
+    for loads in ("", "group"):
         os.environ["PENTA_TMEM_LOADS"] = loads
         plans = [ps.Plan(grids, axis) for axis in range(3)]
         ms = timed(lambda: [pl.execute() for pl in plans], reps=reps, warmup=2)

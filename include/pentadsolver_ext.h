@@ -257,6 +257,9 @@ EXTERN_C PENTAD_API pentadStatus_t pentadsolver_adi_destroy(pentadsolver_adi_t a
  * PENTADSOLVER_SERVE_SEQUENTIAL solves one request at a time (the baseline).
  * Completed requests are read with pentadsolver_server_poll, each with the
  * status bits of its batch (as pentadsolver_status_check reports them).
+ * The server's streams are non-blocking: work that writes a request's arrays
+ * must have completed before the progress call that launches it.  At most
+ * min(n_streams, max_in_flight) batches run at once, one per stream.
  * Not thread-safe: drive one server from one thread. */
 typedef struct pentadsolver_server_s *pentadsolver_server_t;
 #define PENTADSOLVER_SERVE_FP64 0

@@ -29,8 +29,12 @@
 // one request at a time, in arrival order, as the baseline.
 //
 // Coefficients and right-hand sides stay where the caller keeps them (device
-// memory); x is solved in place.  The handle is not thread-safe: submit,
-// progress and poll from one thread, or serialise them.
+// memory); x is solved in place.  The server's streams are non-blocking: work
+// that writes a request's arrays must have completed before the
+// pentadsolver_server_progress call that launches it.  Each batch runs on a
+// stream of its own (at most one batch per stream in flight).  The handle is
+// not thread-safe: submit, progress and poll from one thread, or serialise
+// them.
 #include <cuda_runtime_api.h>
 
 #include <algorithm>
@@ -103,6 +107,7 @@ struct Batch {
   std::vector<Req> reqs;
   pentadsolver_plan_t plan = nullptr;
   size_t off = 0, bytes = 0;
+  size_t stream_index = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
 };
@@ -114,6 +119,7 @@ struct pentadsolver_server_s {
   unsigned char *base = nullptr;
   Arena arena{0};
   std::vector<cudaStream_t> streams;
+  std::vector<char> stream_busy;  // a batch in flight on it
   size_t next_stream = 0;
   int max_batch = 64, max_in_flight = 3, refine_steps = 1, policy = 0;
   bool refine_pays[3] = {true, true, true};
@@ -171,6 +177,7 @@ pentadStatus_t complete_ready(pentadsolver_server_t s, bool wait) {
     pentadsolver_plan_destroy(b.plan);
     cudaEventDestroy(b.done);
     s->arena.release(b.off, b.bytes);
+    s->stream_busy[b.stream_index] = 0;
     for (const Req &r : b.reqs) s->completed.emplace_back(r.id, bits);
     s->in_flight.erase(s->in_flight.begin() + (long)i);
   }
@@ -180,6 +187,17 @@ pentadStatus_t complete_ready(pentadsolver_server_t s, bool wait) {
 // Launch batches while there is room on the device and in the arena.
 pentadStatus_t launch_ready(pentadsolver_server_t s) {
   while (!s->queue.empty() && (int)s->in_flight.size() < s->max_in_flight) {
+    // a stream with nothing in flight: a batch never queues behind another,
+    // and its completion (event, status read) waits for itself only
+    size_t si = s->streams.size();
+    for (size_t k = 0; k < s->streams.size(); ++k) {
+      const size_t c = (s->next_stream + k) % s->streams.size();
+      if (!s->stream_busy[c]) {
+        si = c;
+        break;
+      }
+    }
+    if (si == s->streams.size()) break;
     const auto key = s->key_of(s->queue.front());
     const int cap = s->policy == PENTADSOLVER_SERVE_SEQUENTIAL ? 1 : s->max_batch;
     std::vector<size_t> idx;
@@ -208,8 +226,9 @@ pentadStatus_t launch_ready(pentadsolver_server_t s) {
     b.reqs = reqs;
     b.off = off;
     b.bytes = bytes;
-    b.stream = s->streams[s->next_stream];
-    s->next_stream = (s->next_stream + 1) % s->streams.size();
+    b.stream_index = si;
+    b.stream = s->streams[si];
+    s->next_stream = (si + 1) % s->streams.size();
     pentadStatus_t st = make_plan(s, reqs, key.second, s->base + off, bytes, &b.plan);
     if (st == PENTAD_STATUS_SUCCESS) st = pentadsolver_plan_execute(b.plan, b.stream);
     if (st == PENTAD_STATUS_SUCCESS &&
@@ -225,6 +244,7 @@ pentadStatus_t launch_ready(pentadsolver_server_t s) {
       return st;
     }
     for (size_t k = idx.size(); k-- > 0;) s->queue.erase(s->queue.begin() + (long)idx[k]);
+    s->stream_busy[si] = 1;
     s->in_flight.push_back(b);
     ++s->batches;
   }
@@ -261,6 +281,8 @@ extern "C" PENTAD_API pentadStatus_t pentadsolver_server_create(
     }
     s->streams.push_back(st);
   }
+  s->stream_busy.assign(s->streams.size(), 0);
+  s->max_in_flight = std::min<int>(s->max_in_flight, (int)s->streams.size());
   *server = s;
   return PENTAD_STATUS_SUCCESS;
 }

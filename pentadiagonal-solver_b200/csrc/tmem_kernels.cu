@@ -1110,7 +1110,7 @@ template <typename F> size_t job_scratch_bytes(const Lines &L, bool contig, int 
 // Returns grp, or 0 when the view does not apply (or bulk copies are forced).
 template <typename F> int group_size(const SolveArgs<F> &a, bool contig) {
   const char *e = std::getenv("PENTA_TMEM_LOADS");
-  if (e != nullptr && !std::strcmp(e, "bulk")) return 0;
+  if (e == nullptr || std::strcmp(e, "group") != 0) return 0;
   if (!bulk_ok<F>(a) || tma_ok<F>(a, contig) || tensor_map_encoder() == nullptr) return 0;
   const long long m = contig ? a.L.n : a.L.inner;
   const long long bytes = m * (long long)sizeof(F);
@@ -1301,19 +1301,23 @@ template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig, int
   return job_scratch_bytes<F>(L, contig, fmode);
 }
 
-// Which stage layout a grid's loads use.  0: TMA tiles (aligned rows or
-// runs) or element copies (PENTA_TMEM_LOADS=element, or arrays not 16-byte
-// aligned).  1: the pitched layout -- for misaligned rows or runs, TMA boxes
-// of the group view (group_size), with the rows or lines outside whole groups
-// fetched by bulk copies of aligned supersets; PENTA_TMEM_LOADS=bulk fetches
-// every tile by bulk copies (for measurement: each cp.async.bulk is a TMA
-// request of 80-144 bytes, and B200's TMA unit takes about one request per 18
-// cycles per SM, 1.2-2.4 TB/s in all).
+// Which stage layout a grid's loads use.  0 (the default): TMA tiles for
+// aligned rows or runs, element copies (cp.async, 8 or 4 bytes) for
+// misaligned ones.  1, the pitched layout, selected for measurement: with
+// PENTA_TMEM_LOADS=group, TMA boxes of the group view (group_size) for
+// misaligned grids, the rows or lines outside whole groups by bulk copies of
+// aligned supersets; with =bulk, every tile of any grid by bulk copies.  On
+// B200 both measured slower than element copies for misaligned grids
+// (255^3 FP64: x 354 / 736 us, y 271 / 388 us against 283 / 235 us): every
+// misaligned 128-byte row spans two or three L2 lines, the group boxes along
+// x re-read their overlap chunk (1.5x DRAM reads under evict-first loads),
+// and each cp.async.bulk is a TMA request of 80-144 bytes, of which the TMA
+// unit takes about one per 18 cycles per SM (1.2-2.4 TB/s in all).
 template <typename F> int tmem_loads(const SolveArgs<F> &a, bool contig) {
   const char *e = std::getenv("PENTA_TMEM_LOADS");
-  if (e != nullptr && !std::strcmp(e, "element")) return 0;
   if (e != nullptr && !std::strcmp(e, "bulk")) return bulk_ok<F>(a) ? 1 : 0;
-  return group_size<F>(a, contig) > 0 ? 1 : 0;
+  if (e != nullptr && !std::strcmp(e, "group")) return group_size<F>(a, contig) > 0 ? 1 : 0;
+  return 0;
 }
 
 template <typename F> int tmem_groups(const SolveArgs<F> &a, bool contig) {

@@ -413,34 +413,41 @@ class NativeServer:
         if st != ps.SUCCESS:
             raise ps.PentadError(st, "server create")
         self._grids = {}   # id -> grid descriptor kept alive until completion
+        # the entry points, typed once
+        ct = ctypes
+        self._submit = ps._typed("pentadsolver_server_submit",
+                                 [ct.c_void_p, ct.POINTER(ps.GridDesc), ct.c_int, ct.c_double,
+                                  ct.POINTER(ct.c_ulonglong)])
+        self._progress = ps._typed("pentadsolver_server_progress", [ct.c_void_p, ct.c_int])
+        self._poll = ps._typed("pentadsolver_server_poll",
+                               [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int,
+                                ct.POINTER(ct.c_int)])
+        self._stats = ps._typed("pentadsolver_server_stats",
+                                [ct.c_void_p, ct.c_void_p, ct.c_int])
+        self._cap = 1024
+        self._ids = (ct.c_ulonglong * self._cap)()
+        self._bits = (ct.c_int * self._cap)()
 
     def submit(self, grid: dict, solvedim: int, tol: float) -> int:
         ct, ps = self.ct, self.ps
         desc = ps._grid_descs([grid])
         rid = ct.c_ulonglong(0)
-        st = ps._typed("pentadsolver_server_submit",
-                       [ct.c_void_p, ct.POINTER(ps.GridDesc), ct.c_int, ct.c_double,
-                        ct.POINTER(ct.c_ulonglong)])(self._srv, desc, int(solvedim), float(tol),
-                                                     ct.byref(rid))
+        st = self._submit(self._srv, desc, int(solvedim), float(tol), ct.byref(rid))
         if st != ps.SUCCESS:
             raise ps.PentadError(st, "server submit")
         self._grids[rid.value] = (desc, grid)
         return int(rid.value)
 
     def progress(self, wait: bool = False) -> None:
-        st = self.ps._typed("pentadsolver_server_progress", [self.ct.c_void_p, self.ct.c_int])(
-            self._srv, 1 if wait else 0)
+        st = self._progress(self._srv, 1 if wait else 0)
         if st != self.ps.SUCCESS:
             raise self.ps.PentadError(st, "server progress")
 
-    def poll(self, capacity: int = 1024) -> list[tuple[int, int]]:
+    def poll(self) -> list[tuple[int, int]]:
         ct = self.ct
-        ids = (ct.c_ulonglong * capacity)()
-        bits = (ct.c_int * capacity)()
+        ids, bits = self._ids, self._bits
         n = ct.c_int(0)
-        st = self.ps._typed("pentadsolver_server_poll",
-                            [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int,
-                             ct.POINTER(ct.c_int)])(self._srv, ids, bits, capacity, ct.byref(n))
+        st = self._poll(self._srv, ids, bits, self._cap, ct.byref(n))
         if st != self.ps.SUCCESS:
             raise self.ps.PentadError(st, "server poll")
         out = [(int(ids[i]), int(bits[i])) for i in range(n.value)]
@@ -450,8 +457,7 @@ class NativeServer:
 
     def stats(self) -> dict:
         vals = (self.ct.c_size_t * 6)()
-        self.ps._typed("pentadsolver_server_stats",
-                       [self.ct.c_void_p, self.ct.c_void_p, self.ct.c_int])(self._srv, vals, 6)
+        self._stats(self._srv, vals, 6)
         keys = ("queued", "in_flight", "arena_used", "arena_peak", "arena_bytes", "batches")
         return dict(zip(keys, (int(v) for v in vals)))
 
@@ -502,10 +508,12 @@ def serve_native(pool: ProblemPool, trace, policy: str, arena_bytes: float, max_
     pending = sorted(tr, key=lambda r: r.arrival)
     by_id, xs, bits = {}, {}, {}
     torch.cuda.synchronize()
+    cur = torch.cuda.current_stream()
     t0 = time.perf_counter()
     i, done = 0, 0
     while done < len(tr):
         now = time.perf_counter() - t0
+        submitted = False
         while i < len(pending) and pending[i].arrival <= now:
             r = pending[i]
             p = pool.items[r.problem]
@@ -517,6 +525,9 @@ def serve_native(pool: ProblemPool, trace, policy: str, arena_bytes: float, max_
             xs[rid] = x
             r.admitted = r.started = now
             i += 1
+            submitted = True
+        if submitted:
+            cur.synchronize()   # the iterates' copies, before the server's streams read them
         srv.progress()
         for rid, b in srv.poll():
             r = by_id[rid]

@@ -390,7 +390,7 @@ MISALIGNED_DIMS = [(33, 17, 9), (255, 7, 5), (17, 255, 3), (9, 7, 255), (50, 13,
 
 
 def _loads_run(co, solvedim, loads, monkeypatch):
-    monkeypatch.setenv("PENTA_TMEM_LOADS", loads)
+    monkeypatch.setenv("PENTA_TMEM_LOADS", loads)   # "" = the default choice
     dv = to_dev(co)
     dirn = direction(3, solvedim)
     with ps.Handle() as h:
@@ -404,13 +404,13 @@ def _loads_run(co, solvedim, loads, monkeypatch):
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 def test_misaligned_grids_bulk_element_and_tma_loads_agree(cuda, dims, dtype, monkeypatch):
     """Rows (x) or runs (y, z) that do not start on 16-byte boundaries: the
-    Tensor-Memory kernel fetches them as TMA boxes of a group view (default:
-    pairs or quadruples of rows / lines are 16-byte periodic; the ones
-    outside whole groups by bulk copies), by element copies
-    (PENTA_TMEM_LOADS=element), or all by bulk copies of aligned supersets
-    (=bulk); aligned rows and runs by TMA tiles.  The same arithmetic runs on
-    the same values whichever way they arrive, so the results are identical
-    bit for bit, and equal the oracle's."""
+    Tensor-Memory kernel fetches them by element copies (default), as TMA
+    boxes of a group view (PENTA_TMEM_LOADS=group: pairs or quadruples of
+    rows / lines are 16-byte periodic; the ones outside whole groups by bulk
+    copies), or all by bulk copies of aligned supersets (=bulk); aligned rows
+    and runs by TMA tiles.  The same arithmetic runs on the same values
+    whichever way they arrive, so the results are identical bit for bit, and
+    equal the oracle's."""
     eb = np.dtype(dtype).itemsize
     co = fixtures.random_dominant(dims, 91, dtype)
     for solvedim in range(3):
@@ -422,14 +422,14 @@ def test_misaligned_grids_bulk_element_and_tma_loads_agree(cuda, dims, dtype, mo
         ref = co["x"].copy()
         oracle.solve(co["ds"], co["dl"], co["d"], co["du"], co["dw"], ref, solvedim)
         x_auto, v_auto = _loads_run(co, solvedim, "", monkeypatch)
-        x_elem, v_elem = _loads_run(co, solvedim, "element", monkeypatch)
+        x_grp, v_grp = _loads_run(co, solvedim, "group", monkeypatch)
         x_bulk, v_bulk = _loads_run(co, solvedim, "bulk", monkeypatch)
-        assert "tmem" in v_auto and "tmem" in v_elem and "tmem" in v_bulk
-        assert ("grp" in v_auto) == (not aligned), (dims, solvedim, v_auto)
-        assert "grp" not in v_elem and "bulk" not in v_elem, v_elem
+        assert "tmem" in v_auto and "tmem" in v_grp and "tmem" in v_bulk
+        assert "grp" not in v_auto and "bulk" not in v_auto, v_auto
+        assert ("grp" in v_grp) == (not aligned), (dims, solvedim, v_grp)
         assert "bulk" in v_bulk, v_bulk
         assert fwd_err(x_auto, ref) <= FWD_TOL[dtype], (dims, solvedim, v_auto)
-        assert np.array_equal(x_auto.view(np.uint8), x_elem.view(np.uint8)), (dims, solvedim)
+        assert np.array_equal(x_auto.view(np.uint8), x_grp.view(np.uint8)), (dims, solvedim)
         assert np.array_equal(x_auto.view(np.uint8), x_bulk.view(np.uint8)), (dims, solvedim)
 
 

@@ -81,6 +81,7 @@ def test_native_server_respects_a_small_arena(cuda):
         rid = srv.submit({**{k: p[k] for k in ("ds", "dl", "d", "du", "dw")}, "x": x},
                          i % 3, 1e-13)
         xs[rid] = (pi, i % 3, x)
+    torch.cuda.synchronize()   # the iterates' copies, before the server's streams read them
     srv.progress(wait=True)
     done = dict(srv.poll())
     st = srv.stats()
@@ -97,11 +98,14 @@ def test_native_server_respects_a_small_arena(cuda):
 
 
 def test_native_server_rejects_a_request_larger_than_its_arena(cuda):
+    import torch
+
     pool = serving.ProblemPool([(128, 128, 64)], seed=51)   # plan scratch of several MB
     srv = serving.NativeServer(1 << 20, "fp64")   # 1 MiB: the grid's plan cannot fit
     p = pool.items[0]
     rid = srv.submit({**{k: p[k] for k in ("ds", "dl", "d", "du", "dw")}, "x": p["b"].clone()},
                      0, 1e-13)
+    torch.cuda.synchronize()
     srv.progress(wait=True)
     assert srv.poll() == [(rid, 1 << 30)]   # PENTADSOLVER_SERVER_REJECTED_BIT
     srv.close()
