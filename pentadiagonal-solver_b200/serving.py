@@ -489,9 +489,13 @@ def serve_native(pool: ProblemPool, trace, policy: str, arena_bytes: float, max_
                  refine_steps: int = 1, keep_results: bool = False, calibrate: bool = False,
                  streams: int = 3):
     """Replay a trace in real time through the library's serving handle:
-    each request is submitted when its arrival time comes (its iterate a copy
-    of the problem's right-hand side), the handle batches and launches, and
-    completions are polled.  Returns (report, results, status bits, trace)."""
+    requests whose arrival time has come are submitted (each with its iterate,
+    a copy of the problem's right-hand side) while fewer than three batches'
+    worth wait in the handle's queue -- the others wait here, as the Python
+    loop's admission holds them, so iterates exist only for requests near the
+    device -- the handle batches and launches, and completions are polled.
+    Latency counts from arrival.  Returns (report, results, status bits,
+    trace)."""
     import copy
 
     import torch
@@ -507,6 +511,7 @@ def serve_native(pool: ProblemPool, trace, policy: str, arena_bytes: float, max_
                              "x": p["b"].clone()})
     pending = sorted(tr, key=lambda r: r.arrival)
     by_id, xs, bits = {}, {}, {}
+    window = 3 * max_batch
     torch.cuda.synchronize()
     cur = torch.cuda.current_stream()
     t0 = time.perf_counter()
@@ -514,7 +519,9 @@ def serve_native(pool: ProblemPool, trace, policy: str, arena_bytes: float, max_
     while done < len(tr):
         now = time.perf_counter() - t0
         submitted = False
-        while i < len(pending) and pending[i].arrival <= now:
+        room = window - srv.stats()["queued"]
+        while i < len(pending) and pending[i].arrival <= now and room > 0:
+            room -= 1
             r = pending[i]
             p = pool.items[r.problem]
             x = p["b"].clone()
