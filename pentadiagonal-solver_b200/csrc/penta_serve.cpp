@@ -26,7 +26,7 @@
 // server measured the refined form faster than plain FP64
 // (pentadsolver_server_calibrate), or everywhere when it was not measured.
 // Tighter requests always run in plain FP64.  The sequential policy solves
-// one request at a time, in arrival order, as the baseline.
+// one request at a time, in arrival order, with the plain call (the baseline).
 //
 // Coefficients and right-hand sides stay where the caller keeps them (device
 // memory); x is solved in place.  The server's streams are non-blocking: work
@@ -137,8 +137,15 @@ struct pentadsolver_server_s {
 
 namespace {
 
+// The sequential baseline solves each request alone with the plain call (the
+// reference-sized buffer from the arena), not as a one-grid plan.
+bool direct(pentadsolver_server_t s) { return s->policy == PENTADSOLVER_SERVE_SEQUENTIAL; }
+
 pentadStatus_t plan_bytes(pentadsolver_server_t s, const std::vector<Req> &reqs, bool refined,
                           size_t *bytes) {
+  if (direct(s))
+    return pentadsolver_buffer_size_ex(s->handle, 8, reqs[0].grid.dims, reqs[0].grid.ndim,
+                                       reqs[0].solvedim, bytes);
   std::vector<pentadsolver_grid_t> g;
   for (const Req &r : reqs) g.push_back(r.grid);
   return refined ? pentadsolver_refine_plan_buffer_size(s->handle, (int)g.size(), g.data(),
@@ -172,9 +179,10 @@ pentadStatus_t complete_ready(pentadsolver_server_t s, bool wait) {
       return PENTAD_STATUS_EXECUTION_FAILED;
     }
     int bits = 0;
-    pentadStatus_t st = pentadsolver_plan_status_check(b.plan, b.stream, &bits);
+    pentadStatus_t st = b.plan ? pentadsolver_plan_status_check(b.plan, b.stream, &bits)
+                               : pentadsolver_status_check(s->handle, b.stream, &bits);
     if (st != PENTAD_STATUS_SUCCESS && st != PENTAD_STATUS_ZERO_PIVOT) return st;
-    pentadsolver_plan_destroy(b.plan);
+    if (b.plan) pentadsolver_plan_destroy(b.plan);
     cudaEventDestroy(b.done);
     s->arena.release(b.off, b.bytes);
     s->stream_busy[b.stream_index] = 0;
@@ -229,8 +237,18 @@ pentadStatus_t launch_ready(pentadsolver_server_t s) {
     b.stream_index = si;
     b.stream = s->streams[si];
     s->next_stream = (si + 1) % s->streams.size();
-    pentadStatus_t st = make_plan(s, reqs, key.second, s->base + off, bytes, &b.plan);
-    if (st == PENTAD_STATUS_SUCCESS) st = pentadsolver_plan_execute(b.plan, b.stream);
+    pentadStatus_t st;
+    if (direct(s)) {  // one request, the plain call
+      const pentadsolver_grid_t &g = reqs[0].grid;
+      st = pentadsolver_D_gpsv_batch_ex(
+          s->handle, static_cast<const double *>(g.ds), static_cast<const double *>(g.dl),
+          static_cast<const double *>(g.d), static_cast<const double *>(g.du),
+          static_cast<const double *>(g.dw), static_cast<double *>(g.x), g.dims, g.ndim,
+          reqs[0].solvedim, s->base + off, bytes, b.stream);
+    } else {
+      st = make_plan(s, reqs, key.second, s->base + off, bytes, &b.plan);
+      if (st == PENTAD_STATUS_SUCCESS) st = pentadsolver_plan_execute(b.plan, b.stream);
+    }
     if (st == PENTAD_STATUS_SUCCESS &&
         (cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming) != cudaSuccess ||
          cudaEventRecord(b.done, b.stream) != cudaSuccess)) {
