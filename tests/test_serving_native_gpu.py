@@ -45,13 +45,17 @@ def _oracle_refs(pool, trace):
     return refs
 
 
-@pytest.mark.parametrize("policy", ["mixed", "fp64", "sequential"])
-def test_native_server_results_against_the_oracle(cuda, policy):
+@pytest.mark.parametrize("policy,calibrate", [("mixed", True), ("mixed", False),
+                                              ("fp64", True), ("sequential", True)])
+def test_native_server_results_against_the_oracle(cuda, policy, calibrate):
+    # uncalibrated, the mixed policy refines every loose request (FP32 sweeps +
+    # FP64 refinement); calibrated on B200 it measures refinement slower and
+    # serves them in FP64
     pool = _pool()
     trace = serving.make_trace(60, math.inf, len(pool.shapes), seed=46)
     rep, results, bits, tr = serving.serve_native(pool, trace, policy, arena_bytes=4e9,
                                                   max_batch=16, keep_results=True,
-                                                  calibrate=True)
+                                                  calibrate=calibrate)
     assert rep["requests"] == 60 and len(results) == 60
     if policy == "sequential":
         assert rep["batches"] == 60
