@@ -117,3 +117,35 @@ class Autotuner:
             g["x"].copy_(s)
         self.save()
         return {"best": {"ctas": ctas}}
+
+
+def main(argv=None) -> None:
+    """Tune from the command line: every candidate's time for each solve
+    direction of one grid, fastest first, recorded in the cache file."""
+    import argparse
+
+    import torch
+
+    ap = argparse.ArgumentParser(description=main.__doc__.split("\n")[0])
+    ap.add_argument("--dims", type=int, nargs="+", required=True, help="t_dims, x first")
+    ap.add_argument("--solvedims", type=int, nargs="+", default=None)
+    ap.add_argument("--dtype", choices=("f64", "f32"), default="f64")
+    ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--cache", default=None, help="tuning table file to load and save")
+    args = ap.parse_args(argv)
+    dtype = torch.float64 if args.dtype == "f64" else torch.float32
+    tuner = Autotuner(cache_path=args.cache, reps=args.reps)
+    ps.tuning_clear()
+    p = problem(args.dims, dtype)
+    for sd in args.solvedims if args.solvedims is not None else range(len(args.dims)):
+        rows = ps.autotune_solve(p["ds"], p["dl"], p["d"], p["du"], p["dw"], p["x"], sd,
+                                 reps=args.reps)
+        print(f"dims {args.dims} {args.dtype} solvedim {sd}:")
+        for r in rows:
+            print(f"  {r['ms'] * 1e3:9.1f} us  {r['label']:12s} {r['variant']}")
+    tuner.save()
+
+
+if __name__ == "__main__":
+    main()
+
