@@ -1234,15 +1234,18 @@ template <typename F, bool CONTIG, int FM, int ST, int XST, int LD> int tmem_occ
 // stages beat three: fewer 64-byte requests in flight per line keep HBM row
 // hits up (measured at 256^3 and 512^3); FP32 along x, with 16 rows a stage,
 // and the strided directions want three.  Strided FP64 with both factors in
-// TMEM takes three read-back stages (the autotuner at 256^3: y 153.5 / z 155.1
-// us against 154.9 / 156.6 with four).  The bulk-load variants (loads = 1)
+// TMEM keeps four read-back stages: the autotuner times three ~1% faster on
+// back-to-back solves of one direction at 256^3 (y 153.5 / z 156.0 against
+// 155.5 / 157.4 us), but in the ADI loop (x, y, z launches overlapping
+// through dependent launches) the y solve measured 0.167 ms with three
+// against 0.157-0.158 ms with four.  The bulk-load variants (loads = 1)
 // have wider stages, so some take fewer of them to fit shared memory.
 #define PENTA_TMEM_CONFIGS(X)   \
   X(double, true, 0, 2, 4, 0)   \
   X(double, true, 0, 3, 4, 0)   \
   X(double, true, 0, 3, 3, 0)   \
-  X(double, false, 0, 3, 3, 0)  \
   X(double, false, 0, 3, 4, 0)  \
+  X(double, false, 0, 3, 3, 0)  \
   X(double, false, 0, 2, 4, 0)  \
   X(double, true, 1, 2, 3, 0)   \
   X(double, true, 1, 3, 2, 0)   \
