@@ -615,8 +615,7 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
           err = launch_tmem<F>(a, mc, ctx.sm_count, stream);
           if (err == cudaSuccess) {
             char vb[96];
-            const char *ld = "";
-            if (mc.loads == 1) ld = tmem_groups<F>(a, contig) > 0 ? " grp" : " bulk";
+            const char *ld = mc.loads == 1 ? tmem_loader<F>(a, contig) : "";
             std::snprintf(vb, sizeof vb, "thomas-pcr:tmem P2 S16 R%d x%d/%d%s%s%s", mc.R,
                           mc.stages, mc.xstages,
                           mc.fmode == 2 ? " fbuf" : mc.fmode == 1 ? " w2s" : "", ld,

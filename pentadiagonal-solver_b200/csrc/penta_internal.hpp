@@ -106,10 +106,10 @@ template <typename F> bool tmem_shape(const Lines &L, bool contig, int &fmode);
 template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig, int fmode);
 template <typename F>
 bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf, int &fmode);
-// The stage layout (TmemConfig::loads) a grid's loads take, and for the
-// pitched layout the group size of its TMA view (0: bulk copies only).
+// The stage layout (TmemConfig::loads) a grid's loads take.
 template <typename F> int tmem_loads(const SolveArgs<F> &a, bool contig);
-template <typename F> int tmem_groups(const SolveArgs<F> &a, bool contig);
+// " grp", " bulk", " chunk" or "" -- which loader fills the stages (variant names)
+template <typename F> const char *tmem_loader(const SolveArgs<F> &a, bool contig);
 template <typename F>
 cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count,
                         cudaStream_t stream);

@@ -223,6 +223,13 @@ __device__ __forceinline__ void cp_async_zfill(void *dst, const void *src, bool 
                "l"(src), "n"(BYTES), "r"(valid ? BYTES : 0)
                : "memory");
 }
+// 16-byte copy global -> shared (L2 only) of which the first `bytes` (0..16)
+// are read and the rest written as zeros; 16-byte aligned addresses.
+__device__ __forceinline__ void cp_async16_bytes(void *dst, const void *src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)),
+               "l"(src), "r"(bytes)
+               : "memory");
+}
 // Arrive on `bar` once all of this thread's earlier cp.async copies have landed
 // (counts as one of the barrier's expected arrivals).
 __device__ __forceinline__ void cp_async_mbar_arrive(uint64_t *bar) {

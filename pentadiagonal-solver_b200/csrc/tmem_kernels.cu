@@ -99,6 +99,7 @@ template <typename F> struct alignas(64) TmemJob {
                         // or lines (x) so that each group is 16-byte periodic; 0: none
   int tail;             // first tile (x) / the run (strided) whose rows or lines lie
                         // outside whole groups: fetched by bulk copies
+  int chunks;           // pitched layout filled by 16-byte cp.async copies (no groups)
 };
 
 namespace {
@@ -254,7 +255,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
   struct Geo {
     const TmemJob<F> *J;
     F *x, *scratch;
-    int n, mt, inner, tpr, n_sys, tile_base, n_tiles, tma, grp, tail;
+    int n, mt, inner, tpr, n_sys, tile_base, n_tiles, tma, grp, tail, chunks;
   };
   auto load_geo = [&](const TmemJob<F> *J, Geo &g) {
     g.J = J;
@@ -270,6 +271,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
     g.tma = J->tma;
     g.grp = J->grp;
     g.tail = J->tail;
+    g.chunks = J->chunks;
   };
   auto tile_coords = [&](const Geo &g, int tile, int &c0, int &c2) {
     if (CONTIG) {
@@ -378,6 +380,51 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
                 }
               }
           }
+        } else if (LD == 1 && JG.chunks) {
+          // 16-byte cp.async copies of the same windows as the bulk copies
+          // below: every row (strided) or line's R rows (x), widened to the
+          // 16-byte chunks that hold them.  Each lane keeps the same (window,
+          // chunk) pairs for every tile half, so a copy costs the stage's row
+          // offset and an add.  A chunk reaching past an array's end is read
+          // only up to it (the rest zero-filled); windows of rows past n (the
+          // lower half's virtual rows) and of lines past the grid are skipped.
+          constexpr int NCH = (CONTIG ? PL : PS) / G::EPC;  // chunks per window
+          constexpr int NW = CONTIG ? TS : R;                // windows per tile half
+          constexpr int NP = NW * NCH;
+          constexpr int KP = (NP + 31) / 32;
+          const long long npts = (long long)n * JG.n_sys;
+#pragma unroll
+          for (int kp = 0; kp < KP; ++kp) {
+            const int p = lane + 32 * kp;
+            if (p >= NP) continue;
+            const int w = p / NCH, j = p - (p / NCH) * NCH;
+            const int doff = w * (CONTIG ? PL : PS) + j * G::EPC;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int r0 = h ? r_dn : r_up;
+              long long off;
+              bool ok;
+              if (CONTIG) {
+                off = (long long)(c0 + w) * n + r0;
+                ok = c0 + w < JG.n_sys && r0 < n;
+              } else {
+                off = (long long)c2 * inner * n + (long long)(r0 + w) * inner + c0;
+                ok = r0 + w < n;
+              }
+              const long long e = (off & ~(long long)(G::EPC - 1)) + j * G::EPC;
+              const long long left = npts - e;
+              const int bytes = !ok || left <= 0
+                                    ? 0
+                                    : (left >= G::EPC ? 16 : (int)(left * (long long)sizeof(F)));
+              if (bytes == 0) continue;
+#pragma unroll
+              for (int q = 0; q < 6; ++q) {
+                const int aq = h ? (q < 5 ? 4 - q : 5) : q;
+                cp_async16_bytes(dst + (2 * q + h) * BOXL + doff, arrs[aq] + e, bytes);
+              }
+            }
+          }
+          cp_async_mbar_arrive(&full[slot]);
         } else if constexpr (LD == 1) {
           // Bulk copies of 16-byte aligned supersets.  Copy k of the stage:
           // tile bx = 2 q + half, then line (along x) or row (strided) `sub`.
@@ -1104,6 +1151,13 @@ template <typename F> size_t job_scratch_bytes(const Lines &L, bool contig, int 
          (fmode == 2 ? 3 : fmode == 1 ? 2 : 1) * sizeof(F);
 }
 
+// The pitched layout filled by 16-byte cp.async copies (PENTA_TMEM_LOADS=chunk;
+// arrays on 16-byte boundaries).
+template <typename F> bool chunk_loads(const SolveArgs<F> &a) {
+  const char *e = std::getenv("PENTA_TMEM_LOADS");
+  return e != nullptr && !std::strcmp(e, "chunk") && bulk_ok<F>(a);
+}
+
 // The group view of a grid whose rows (x) or runs (strided) are not 16-byte
 // aligned: `grp` consecutive lines (x) or rows (strided) form a 16-byte
 // periodic group, so maps over {grp * stride, groups} are valid tensor maps.
@@ -1156,7 +1210,10 @@ bool fill_job(TmemJob<F> &J, const SolveArgs<F> &a, bool contig, F *scratch, int
   if (J.tma && contig && !encode<F>(&J.maps[6], a.x, a.L, contig, R, true)) J.tma = 0;
   J.grp = 0;
   J.tail = contig ? 0x7fffffff : -1;
-  if (loads == 1) {  // pitched layout: the group view where it applies
+  J.chunks = 0;
+  if (loads == 1 && chunk_loads<F>(a)) {
+    J.chunks = 1;
+  } else if (loads == 1) {  // pitched layout: the group view where it applies
     const int g = group_size<F>(a, contig);
     bool ok = g > 0;
     for (int q = 0; ok && q < 6; ++q) ok = encode_groups<F>(&J.maps[q], ptrs[q], a.L, contig, g, R);
@@ -1322,11 +1379,15 @@ template <typename F> int tmem_loads(const SolveArgs<F> &a, bool contig) {
   const char *e = std::getenv("PENTA_TMEM_LOADS");
   if (e != nullptr && !std::strcmp(e, "bulk")) return bulk_ok<F>(a) ? 1 : 0;
   if (e != nullptr && !std::strcmp(e, "group")) return group_size<F>(a, contig) > 0 ? 1 : 0;
+  if (e != nullptr && !std::strcmp(e, "chunk"))
+    return (chunk_loads<F>(a) && !tma_ok<F>(a, contig)) ? 1 : 0;
   return 0;
 }
 
-template <typename F> int tmem_groups(const SolveArgs<F> &a, bool contig) {
-  return tmem_loads<F>(a, contig) == 1 ? group_size<F>(a, contig) : 0;
+template <typename F> const char *tmem_loader(const SolveArgs<F> &a, bool contig) {
+  if (tmem_loads<F>(a, contig) != 1) return "";
+  if (chunk_loads<F>(a)) return " chunk";
+  return group_size<F>(a, contig) > 0 ? " grp" : " bulk";
 }
 
 template <typename F>
@@ -1455,8 +1516,8 @@ template bool tmem_fill_jobs<double>(const SolveArgs<double> *, int, bool, int, 
                                      unsigned char *, void *, size_t *, int *);
 template bool tmem_fill_jobs<float>(const SolveArgs<float> *, int, bool, int, int,
                                     unsigned char *, void *, size_t *, int *);
-template int tmem_groups<double>(const SolveArgs<double> &, bool);
-template int tmem_groups<float>(const SolveArgs<float> &, bool);
+template const char *tmem_loader<double>(const SolveArgs<double> &, bool);
+template const char *tmem_loader<float>(const SolveArgs<float> &, bool);
 template cudaError_t launch_tmem_batch<double>(const void *, int, int, bool, int, int, bool,
                                                int, int *, cudaStream_t);
 template cudaError_t launch_tmem_batch<float>(const void *, int, int, bool, int, int, bool, int,
