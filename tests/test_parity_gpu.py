@@ -407,8 +407,9 @@ def test_misaligned_grids_bulk_element_and_tma_loads_agree(cuda, dims, dtype, mo
     Tensor-Memory kernel fetches them by element copies (default), as TMA
     boxes of a group view (PENTA_TMEM_LOADS=group: pairs or quadruples of
     rows / lines are 16-byte periodic; the ones outside whole groups by bulk
-    copies), or all by bulk copies of aligned supersets (=bulk); aligned rows
-    and runs by TMA tiles.  The same arithmetic runs on the same values
+    copies), by 16-byte cp.async copies of aligned supersets (=chunk), or all
+    by bulk copies of aligned supersets (=bulk); aligned rows and runs by TMA
+    tiles.  The same arithmetic runs on the same values
     whichever way they arrive, so the results are identical bit for bit, and
     equal the oracle's."""
     eb = np.dtype(dtype).itemsize
@@ -424,6 +425,9 @@ def test_misaligned_grids_bulk_element_and_tma_loads_agree(cuda, dims, dtype, mo
         x_auto, v_auto = _loads_run(co, solvedim, "", monkeypatch)
         x_grp, v_grp = _loads_run(co, solvedim, "group", monkeypatch)
         x_bulk, v_bulk = _loads_run(co, solvedim, "bulk", monkeypatch)
+        x_chk, v_chk = _loads_run(co, solvedim, "chunk", monkeypatch)
+        assert ("chunk" in v_chk) == (not aligned), (dims, solvedim, v_chk)
+        assert np.array_equal(x_auto.view(np.uint8), x_chk.view(np.uint8)), (dims, solvedim)
         assert "tmem" in v_auto and "tmem" in v_grp and "tmem" in v_bulk
         assert "grp" not in v_auto and "bulk" not in v_auto, v_auto
         assert ("grp" in v_grp) == (not aligned), (dims, solvedim, v_grp)
