@@ -24,9 +24,9 @@
 
   odd      odd-size grids: each axis of 255^3 against 256^3, FP64 and FP32, timed as
            single solves (CUDA events, 7 x 930 MB per axis: above L2, no flush),
-           with the misaligned rows / runs loaded by element copies (default),
-           group-view TMA boxes (PENTA_TMEM_LOADS=group) and 16-byte cp.async
-           chunks (=chunk), aligned 256^3 also by bulk copies (=bulk), and the
+           with the misaligned rows / runs loaded by 16-byte cp.async chunks
+           (default), element copies (PENTA_TMEM_LOADS=element) and group-view
+           TMA boxes (=group), aligned 256^3 also by bulk copies (=bulk), and the
            16 smallest of config 3's grids as FP64 plans; GB/s of 7 sizeof(F) B
            per point.
 
@@ -418,7 +418,7 @@ def config_odd(reps=10):
                 dims = (edge, edge, edge)
                 p = dev_problem(dims, 7, dtype)
                 b = p["x"].clone()
-                for loads in ("", "group", "chunk"):
+                for loads in ("", "element", "group"):
                     if loads and edge % (16 // eb) == 0:
                         continue   # aligned: TMA tiles either way
                     os.environ["PENTA_TMEM_LOADS"] = loads
@@ -448,7 +448,7 @@ def config_odd(reps=10):
     sub = sorted(dims_list, key=math.prod)[:16]
     grids = [dev_problem(d, 500 + i) for i, d in enumerate(sub)]
     pts = sum(math.prod(d) for d in sub)
-    for loads in ("", "group", "chunk"):
+    for loads in ("", "element", "group"):
         os.environ["PENTA_TMEM_LOADS"] = loads
         plans = [ps.Plan(grids, axis) for axis in range(3)]
         ms = timed(lambda: [pl.execute() for pl in plans], reps=reps, warmup=2)

@@ -1151,11 +1151,15 @@ template <typename F> size_t job_scratch_bytes(const Lines &L, bool contig, int 
          (fmode == 2 ? 3 : fmode == 1 ? 2 : 1) * sizeof(F);
 }
 
-// The pitched layout filled by 16-byte cp.async copies (PENTA_TMEM_LOADS=chunk;
-// arrays on 16-byte boundaries).
+// The pitched layout filled by 16-byte cp.async copies: the default for
+// misaligned rows or runs whose arrays start on 16-byte boundaries, unless
+// PENTA_TMEM_LOADS names another loader.
 template <typename F> bool chunk_loads(const SolveArgs<F> &a) {
   const char *e = std::getenv("PENTA_TMEM_LOADS");
-  return e != nullptr && !std::strcmp(e, "chunk") && bulk_ok<F>(a);
+  if (e != nullptr && (!std::strcmp(e, "bulk") || !std::strcmp(e, "group") ||
+                       !std::strcmp(e, "element")))
+    return false;
+  return bulk_ok<F>(a);
 }
 
 // The group view of a grid whose rows (x) or runs (strided) are not 16-byte
@@ -1363,25 +1367,27 @@ template <typename F> size_t tmem_scratch_bytes(const Lines &L, bool contig, int
   return job_scratch_bytes<F>(L, contig, fmode);
 }
 
-// Which stage layout a grid's loads use.  0 (the default): TMA tiles for
-// aligned rows or runs, element copies (cp.async, 8 or 4 bytes) for
-// misaligned ones.  1, the pitched layout, selected for measurement: with
-// PENTA_TMEM_LOADS=group, TMA boxes of the group view (group_size) for
-// misaligned grids, the rows or lines outside whole groups by bulk copies of
-// aligned supersets; with =bulk, every tile of any grid by bulk copies.  On
-// B200 both measured slower than element copies for misaligned grids
-// (255^3 FP64: x 354 / 736 us, y 271 / 388 us against 283 / 235 us): every
-// misaligned 128-byte row spans two or three L2 lines, the group boxes along
-// x re-read their overlap chunk (1.5x DRAM reads under evict-first loads),
-// and each cp.async.bulk is a TMA request of 80-144 bytes, of which the TMA
-// unit takes about one per 18 cycles per SM (1.2-2.4 TB/s in all).
+// Which stage layout a grid's loads use.  0: TMA tiles for aligned rows or
+// runs; element copies (cp.async, 8 or 4 bytes) for misaligned ones whose
+// arrays do not start on 16-byte boundaries, or with
+// PENTA_TMEM_LOADS=element.  1, the pitched layout (one 16-byte chunk wider
+// per row or line): by default for misaligned rows or runs, filled by
+// 16-byte cp.async copies of the aligned superset of each row or line
+// (chunk_loads; 255^3 FP64 x 229, y 177, z 183 us against 284 / 237 / 241
+// with element copies -- a quarter to a half of their copy instructions).
+// For measurement: PENTA_TMEM_LOADS=group fills it with TMA boxes of the
+// group view (group_size), =bulk with one cp.async.bulk per row or line (any
+// grid).  Both measured slower than element copies (255^3 FP64: x 354 / 736
+// us, y 271 / 388 us): every misaligned 128-byte row spans two or three L2
+// lines, the group boxes along x re-read their overlap chunk (1.5x DRAM reads
+// under evict-first loads), and each cp.async.bulk is a TMA request of 80-144
+// bytes, of which the TMA unit takes about one per 18 cycles per SM.
 template <typename F> int tmem_loads(const SolveArgs<F> &a, bool contig) {
   const char *e = std::getenv("PENTA_TMEM_LOADS");
   if (e != nullptr && !std::strcmp(e, "bulk")) return bulk_ok<F>(a) ? 1 : 0;
   if (e != nullptr && !std::strcmp(e, "group")) return group_size<F>(a, contig) > 0 ? 1 : 0;
-  if (e != nullptr && !std::strcmp(e, "chunk"))
-    return (chunk_loads<F>(a) && !tma_ok<F>(a, contig)) ? 1 : 0;
-  return 0;
+  if (e != nullptr && !std::strcmp(e, "element")) return 0;
+  return (chunk_loads<F>(a) && !tma_ok<F>(a, contig)) ? 1 : 0;
 }
 
 template <typename F> const char *tmem_loader(const SolveArgs<F> &a, bool contig) {

@@ -404,11 +404,11 @@ def _loads_run(co, solvedim, loads, monkeypatch):
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 def test_misaligned_grids_bulk_element_and_tma_loads_agree(cuda, dims, dtype, monkeypatch):
     """Rows (x) or runs (y, z) that do not start on 16-byte boundaries: the
-    Tensor-Memory kernel fetches them by element copies (default), as TMA
-    boxes of a group view (PENTA_TMEM_LOADS=group: pairs or quadruples of
-    rows / lines are 16-byte periodic; the ones outside whole groups by bulk
-    copies), by 16-byte cp.async copies of aligned supersets (=chunk), or all
-    by bulk copies of aligned supersets (=bulk); aligned rows and runs by TMA
+    Tensor-Memory kernel fetches them by 16-byte cp.async copies of aligned
+    supersets (default), by element copies (PENTA_TMEM_LOADS=element), as TMA
+    boxes of a group view (=group: pairs or quadruples of rows / lines are
+    16-byte periodic; the ones outside whole groups by bulk copies), or all by
+    bulk copies of aligned supersets (=bulk); aligned rows and runs by TMA
     tiles.  The same arithmetic runs on the same values
     whichever way they arrive, so the results are identical bit for bit, and
     equal the oracle's."""
@@ -425,11 +425,11 @@ def test_misaligned_grids_bulk_element_and_tma_loads_agree(cuda, dims, dtype, mo
         x_auto, v_auto = _loads_run(co, solvedim, "", monkeypatch)
         x_grp, v_grp = _loads_run(co, solvedim, "group", monkeypatch)
         x_bulk, v_bulk = _loads_run(co, solvedim, "bulk", monkeypatch)
-        x_chk, v_chk = _loads_run(co, solvedim, "chunk", monkeypatch)
-        assert ("chunk" in v_chk) == (not aligned), (dims, solvedim, v_chk)
-        assert np.array_equal(x_auto.view(np.uint8), x_chk.view(np.uint8)), (dims, solvedim)
+        x_elm, v_elm = _loads_run(co, solvedim, "element", monkeypatch)
+        assert "chunk" not in v_elm and "grp" not in v_elm and "bulk" not in v_elm, v_elm
+        assert np.array_equal(x_auto.view(np.uint8), x_elm.view(np.uint8)), (dims, solvedim)
         assert "tmem" in v_auto and "tmem" in v_grp and "tmem" in v_bulk
-        assert "grp" not in v_auto and "bulk" not in v_auto, v_auto
+        assert ("chunk" in v_auto) == (not aligned), (dims, solvedim, v_auto)
         assert ("grp" in v_grp) == (not aligned), (dims, solvedim, v_grp)
         assert "bulk" in v_bulk, v_bulk
         assert fwd_err(x_auto, ref) <= FWD_TOL[dtype], (dims, solvedim, v_auto)
