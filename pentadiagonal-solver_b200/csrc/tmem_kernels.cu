@@ -140,7 +140,10 @@ template <typename F, bool CONTIG, int FM, int ST, int XST, int LD> struct TmemG
     return ((kRows / g) * kPitch * (int)sizeof(F) + 127) / 128 * 128 / (int)sizeof(F);
   }
   static constexpr int CP2 = cls(2), CP4 = cls(4);
-  static constexpr int kPitched0 = kRows * kPitch;
+  // along x, lines 8-15 of a tile sit one chunk further (line_off): lines l
+  // and l + 8 would otherwise start on the same banks with the same shift
+  __host__ __device__ static constexpr int line_off(int l) { return l * PL + (l >= 8 ? EPC : 0); }
+  static constexpr int kPitched0 = kRows * kPitch + (CONTIG ? EPC : 0);
   static constexpr int kPitched1 = 2 * CP2 > kPitched0 ? 2 * CP2 : kPitched0;
   static constexpr int kPitched =
       (sizeof(F) == 4 && 4 * CP4 > kPitched1) ? 4 * CP4 : kPitched1;  // FP32 groups of 4
@@ -398,7 +401,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
             const int p = lane + 32 * kp;
             if (p >= NP) continue;
             const int w = p / NCH, j = p - (p / NCH) * NCH;
-            const int doff = w * (CONTIG ? PL : PS) + j * G::EPC;
+            const int doff = (CONTIG ? G::line_off(w) : w * PS) + j * G::EPC;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
               const int r0 = h ? r_dn : r_up;
@@ -467,7 +470,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
               cnt = row < n ? min(TS, inner - c0) : 0;
               off = (long long)c2 * inner * n + (long long)row * inner + c0;
             }
-            F *const tdst = dst + bx * BOXL + sub * (CONTIG ? PL : PS);
+            F *const tdst = dst + bx * BOXL + (CONTIG ? G::line_off(sub) : sub * PS);
             nbs[kk] = 0;
             if (cnt > 0) {
               const long long first = off & ~(long long)(EPC - 1);
@@ -646,7 +649,7 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
           const int sh = (int)(((long long)(c0 + sys) * n) & (G::EPC - 1));
 #pragma unroll
           for (int r = 0; r < R; ++r)
-            ldm[r] = part * BOXL + sys * PL + sh + (part ? (R - 1 - r) : r);
+            ldm[r] = part * BOXL + G::line_off(sys) + sh + (part ? (R - 1 - r) : r);
         } else {
           const int s0 = (int)(((long long)c2 * JG.inner * n) & (G::EPC - 1));
           const int im = JG.inner & (G::EPC - 1);
@@ -1324,9 +1327,9 @@ template <typename F, bool CONTIG, int FM, int ST, int XST, int LD> int tmem_occ
   X(float, false, 2, 3, 2, 0)   \
   X(double, true, 0, 2, 4, 1)   \
   X(double, false, 0, 3, 3, 1)  \
-  X(double, true, 1, 2, 3, 1)   \
+  X(double, true, 1, 2, 2, 1)   \
   X(double, false, 1, 2, 4, 1)  \
-  X(double, true, 2, 2, 2, 1)   \
+  X(double, true, 2, 2, 1, 1)   \
   X(double, false, 2, 2, 2, 1)  \
   X(float, true, 0, 2, 4, 1)    \
   X(float, false, 0, 2, 4, 1)   \
