@@ -31,6 +31,8 @@ one implementation of it.
 """
 from __future__ import annotations
 
+import contextlib
+import gc
 import math
 import time
 from dataclasses import dataclass, field
@@ -73,6 +75,20 @@ def make_trace(n_requests: int, rate: float, n_problems: int, seed: int,
         out.append(Request(i, t, int(rng.integers(n_problems)), int(rng.integers(3)),
                            1e-10 if rng.random() < frac_loose else 1e-13))
     return out
+
+
+@contextlib.contextmanager
+def no_gc():
+    """Python's cyclic garbage collector paused while a trace is served, so
+    that its pauses do not land in the latencies (it runs once afterwards)."""
+    enabled = gc.isenabled()
+    gc.disable()
+    try:
+        yield
+    finally:
+        if enabled:
+            gc.enable()
+        gc.collect()
 
 
 def percentile(values, q):
@@ -366,9 +382,10 @@ def serve(pool: ProblemPool, trace, policy: str, budget_bytes: float, max_batch:
     sch = Scheduler(ex, budget_bytes, max_batch=max_batch,
                     max_in_flight=1 if policy == "sequential" else 3, policy=policy)
     ex.torch.cuda.synchronize()
-    ex.t0 = time.perf_counter()
-    sch.run(tr)
-    ex.torch.cuda.synchronize()
+    with no_gc():
+        ex.t0 = time.perf_counter()
+        sch.run(tr)
+        ex.torch.cuda.synchronize()
     rep = report(tr)
     rep.update({"policy": policy, "batches": sch.batches,
                 "peak_budget_gb": round(sch.peak / 1e9, 3)})
@@ -514,6 +531,8 @@ def serve_native(pool: ProblemPool, trace, policy: str, arena_bytes: float, max_
     window = 3 * max_batch
     torch.cuda.synchronize()
     cur = torch.cuda.current_stream()
+    gc_ctx = no_gc()
+    gc_ctx.__enter__()
     t0 = time.perf_counter()
     i, done = 0, 0
     while done < len(tr):
@@ -548,6 +567,7 @@ def serve_native(pool: ProblemPool, trace, policy: str, arena_bytes: float, max_
             if dt > 2e-4:
                 time.sleep(dt - 1e-4)
     torch.cuda.synchronize()
+    gc_ctx.__exit__(None, None, None)
     rep = report(tr)
     st = srv.stats()
     rep.update({"policy": policy, "native": True, "batches": st["batches"],
