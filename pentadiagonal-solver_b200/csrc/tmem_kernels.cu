@@ -979,19 +979,28 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
           // misaligned grid (no TMA): the step's results go through the
           // shared tile and leave in runs of a line's R rows, R consecutive
           // lanes a run, instead of one scattered element per lane
+          // (lane: row rr = lane % R of lines a + (32 / R) j, one pointer
+          // step a line group; the rows of each half checked once)
           F *const ob = obuf;
 #pragma unroll
           for (int r = 0; r < R; ++r) ob[st1[r]] = xk[r];
           __syncwarp();
-#pragma unroll 4
-          for (int k = 0; k < 2 * BOX / 32; ++k) {
-            const int idx = lane + 32 * k;
-            const int h = idx / BOX, rem = idx - h * BOX;
-            const int l = rem / R, rr = rem - l * R;
+          constexpr int LPI = 32 / R;  // lines a warp instruction writes
+          const int a0 = lane / R, rr = lane % R;
+          F *const xl = JG.x + (long long)(c0 + a0) * n;
+          const long long lstep = (long long)LPI * n;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
             const int row = h ? (mt + s * R + rr) : (mt - (s + 1) * R + rr);
-            if (row < n && c0 + l < JG.n_sys)
-              JG.x[(long long)(c0 + l) * n + row] =
-                  ob[h * 2 * BOX + l * R + ((rr / EPC) ^ ((l >> 1) & 3)) * EPC + rr % EPC];
+            if (row < n) {
+#pragma unroll
+              for (int j = 0; j < TS / LPI; ++j) {
+                const int l = a0 + LPI * j;
+                if (c0 + l < JG.n_sys)
+                  xl[j * lstep + row] =
+                      ob[h * 2 * BOX + l * R + ((rr / EPC) ^ ((l >> 1) & 3)) * EPC + rr % EPC];
+              }
+            }
           }
           __syncwarp();
         } else if (CONTIG) {
