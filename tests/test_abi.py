@@ -143,3 +143,33 @@ def test_headers_compile_as_c_and_cpp(tmp_path):
                     str(tmp_path / "t3.o")], check=True)
     subprocess.run([cxx, "-std=c++17", "-Wall", "-Werror", f"-I{INCLUDE}", "-x", "c++", "-c",
                     str(src2), "-o", str(tmp_path / "t4.o")], check=True)
+
+
+def test_adi_graph_refuses_bad_arguments_before_touching_a_device():
+    # pentadsolver_adi_create checks its arguments before any device work
+    # (NULL out-pointer, element size, missing arrays or buffer, iteration
+    # count, a buffer smaller than the x direction's reference size)
+    import ctypes
+
+    import pentadsolver as ps
+
+    f = ps._typed("pentadsolver_adi_create",
+                  [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 7 +
+                  [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
+                   ctypes.POINTER(ctypes.c_void_p)])
+    out = ctypes.c_void_p(None)
+    dims = ps._dims([16, 16, 16])
+    need = ps.buffer_size([16, 16, 16], 0, 8)
+    arrs = [256] * 6
+    cases = [
+        (8, arrs, 3, 1, 256, need, None),           # no out-pointer
+        (2, arrs, 3, 1, 256, need, out),            # element size
+        (8, [256] * 5 + [0], 3, 1, 256, need, out),  # missing x
+        (8, arrs, 3, 0, 256, need, out),            # no iterations
+        (8, arrs, 3, 1, 0, need, out),              # no buffer
+        (8, arrs, 3, 1, 256, need - 8, out),        # buffer too small
+    ]
+    for eb, a, nd, it, buf, nbytes, o in cases:
+        st = f(None, eb, *a, dims, nd, it, buf, nbytes, None if o is None else ctypes.byref(o))
+        assert st == ps.INVALID_VALUE, (eb, nd, it, buf, nbytes)
+        assert not out.value
