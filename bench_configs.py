@@ -12,6 +12,8 @@
            the three captured in one CUDA graph; FP64 and FP32 + 1 refinement
            step (all 96 grids); against per-grid single calls.  Forward errors
            of both forms against the CPU oracle, grid by grid.
+  3split   config 3's FP64 plans per axis and bucket of line length along it (32-64
+           ... 321-384, and all): where the time goes.
   config4  serving: a Poisson stream (2000 requests/s) of grids with per-axis
            N ~ logU[16, 512] from a device-resident pool, solvedim U{0,1,2},
            70% at tolerance 1e-10 and 30% at 1e-13, 150 GB budget; p50/p99
@@ -55,7 +57,7 @@ bench.py, this script uses oracle/ only as the checker (forward errors) and
 for the reference's own CPU code timed as the baseline; the solves and grids
 it measures are the library's.
 
-  python bench_configs.py [--configs 0,2,3,4,odd,mesh,refapp]
+  python bench_configs.py [--configs 0,2,3,3split,4,odd,mesh,refapp]
 """
 from __future__ import annotations
 
@@ -402,6 +404,35 @@ def config4(rate=2000.0, seconds=2.0, n_problems=64, budget=150e9, seed=44):
     return out
 
 
+def config3_split(n_grids=96, lo=32, hi=384, seed=33):
+    """Config 3's FP64 plans broken down: per axis, one plan per bucket of line
+    length along that axis (n <= 256: du2 and dw2 in Tensor Memory; n > 256:
+    dw2 with x2 through the buffer)."""
+    import torch
+
+    import pentadsolver as ps
+
+    rng = np.random.default_rng(seed)
+    dims_list = [tuple(int(v) for v in rng.integers(lo, hi + 1, size=3)) for _ in range(n_grids)]
+    grids = [dev_problem(d, 1000 + i) for i, d in enumerate(dims_list)]
+    out = {"config": "config3_split", "grids": n_grids, "seed": seed, "rows": []}
+    buckets = ((32, 64), (65, 128), (129, 192), (193, 256), (257, 320), (321, 384))
+    for axis in range(3):
+        for b0, b1 in buckets + ((lo, hi),):
+            idx = [i for i in range(n_grids) if b0 <= dims_list[i][axis] <= b1]
+            if not idx:
+                continue
+            pts = sum(math.prod(dims_list[i]) for i in idx)
+            with ps.Plan([grids[i] for i in idx], axis) as pl:
+                ms = timed(lambda: pl.execute(), reps=5, warmup=2)
+            out["rows"].append({"axis": axis, "n": [b0, b1], "grids": len(idx),
+                                "Mpts": round(pts / 1e6, 1), "ms": round(ms, 3),
+                                "GBps": round(56 * pts / ms / 1e6, 1)})
+            torch.cuda.synchronize()
+    out["peak_GBps"] = peak()
+    return out
+
+
 def config_odd(reps=10):
     import os
 
@@ -585,10 +616,11 @@ def main():
     want = {c.strip() for c in args.configs.split(",")}
     runs = {"0": config0, "2": lambda: config2(args.n2), "3": lambda: config3(args.grids3),
             "4": lambda: config4(seconds=args.seconds4), "mesh": config_mesh,
-            "refapp": config_refapp, "odd": lambda: config_odd(args.odd_reps)}
+            "refapp": config_refapp, "odd": lambda: config_odd(args.odd_reps),
+            "3split": config3_split}
     from bench import ClockSampler
 
-    for c in ("0", "2", "3", "4", "odd", "mesh", "refapp"):
+    for c in ("0", "2", "3", "3split", "4", "odd", "mesh", "refapp"):
         if c in want:
             t0 = time.time()
             with ClockSampler(0) as clk:
