@@ -147,7 +147,9 @@ EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_destroy(pentadsolver_plan_t
  * buffer (from an earlier call with the same coefficients) are used as they
  * are.  The buffer's first 16 bytes receive (max|last correction|, max|x|)
  * of the last step, an estimate of the remaining forward error
- * (pentadsolver_refine_estimate reads them). */
+ * (pentadsolver_refine_estimate reads them; zeros when steps = 0).  With
+ * steps <= 1 the first iterate stays in FP32 and b in x until the result is
+ * written (no FP64 copies of either): fewer bytes, the same values. */
 EXTERN_C PENTAD_API pentadStatus_t pentadsolver_refine_buffer_size(
     pentadsolver_handle_t handle, const int *t_dims, int t_ndim, int t_solvedim, size_t *bytes);
 EXTERN_C PENTAD_API pentadStatus_t pentadsolver_D_gpsv_batch_refine(

@@ -743,11 +743,14 @@ struct Plan {
   double *est = nullptr;         // device [count][2]
   int count = 0;
   Plan *fp32 = nullptr;          // the FP32 plan over the cast copies
+  Plan *fp32q = nullptr;         // the same over the q arrays (one-step form)
+  bool owns_slot = true;         // false: fp32q reports into fp32's slot
   // the slot the plan's kernels report into (a refine plan's FP32 sweeps)
   int report_slot() const { return fp32 ? fp32->slot : slot; }
   ~Plan() {
+    delete fp32q;
     delete fp32;
-    if (ctx) status_slot_release(slot, ctx->device);
+    if (ctx && owns_slot) status_slot_release(slot, ctx->device);
   }
 };
 
@@ -1001,6 +1004,7 @@ RefineGrid refine_grid(const Shape &sh, const double *ds, const double *dl, cons
   g.b = b;
   g.s_ds = s; g.s_dl = s + N; g.s_d = s + 2 * N; g.s_du = s + 3 * N; g.s_dw = s + 4 * N;
   g.r = r;
+  g.q = reinterpret_cast<float *>(b);  // one-step form: b is not copied, its slot holds q
   g.est = est;
   g.n_points = (long long)N;
   g.n = (int)sh.L.n;
@@ -1041,16 +1045,28 @@ pentadStatus_t refine_solve(Context &ctx, const double *ds, const double *dl, co
   auto step = [&](RefineStep k) {
     return launch_refine_step(k, g, nullptr, 1, chunks, stream) == cudaSuccess;
   };
-  auto sweep = [&]() {
-    return solve<float>(ctx, g.s_ds, g.s_dl, g.s_d, g.s_du, g.s_dw, g.r, dims, ndim, solvedim,
+  auto sweep = [&](float *rhs) {
+    return solve<float>(ctx, g.s_ds, g.s_dl, g.s_d, g.s_du, g.s_dw, rhs, dims, ndim, solvedim,
                         base + l.solve, l.total - l.solve, stream, why);
   };
+  if (steps <= 1) {  // the one-step form: no FP64 copies of x0 and b
+    if (!step(reuse ? RefineStep::First : RefineStep::FirstCast)) goto failed;
+    if ((st = sweep(g.r)) != PENTAD_STATUS_SUCCESS) return st;
+    if (steps == 0) {
+      if (!step(RefineStep::Lift)) goto failed;
+      return PENTAD_STATUS_SUCCESS;
+    }
+    if (!step(RefineStep::Residual1)) goto failed;
+    if ((st = sweep(g.q)) != PENTAD_STATUS_SUCCESS) return st;
+    if (!step(RefineStep::Correct1)) goto failed;
+    return PENTAD_STATUS_SUCCESS;
+  }
   if (!step(reuse ? RefineStep::Prepare : RefineStep::PrepareCast)) goto failed;
-  if ((st = sweep()) != PENTAD_STATUS_SUCCESS) return st;
+  if ((st = sweep(g.r)) != PENTAD_STATUS_SUCCESS) return st;
   if (!step(RefineStep::Lift)) goto failed;
   for (int k = 0; k < steps; ++k) {
     if (!step(RefineStep::Residual)) goto failed;
-    if ((st = sweep()) != PENTAD_STATUS_SUCCESS) return st;
+    if ((st = sweep(g.r)) != PENTAD_STATUS_SUCCESS) return st;
     if (!step(RefineStep::Correct)) goto failed;
   }
   return PENTAD_STATUS_SUCCESS;
@@ -1083,10 +1099,12 @@ pentadStatus_t refine_plan_layout(int count, const pentadsolver_grid_t *grids, i
   return PENTAD_STATUS_SUCCESS;
 }
 
-// The FP32 grids of a refine plan (the cast coefficients and r).
+// The FP32 grids of a refine plan (the cast coefficients and r, or with
+// `on_q` the q array in the slot of b).
 void refine_fp32_grids(int count, const pentadsolver_grid_t *grids,
                        const std::vector<Shape> &shapes, const std::vector<size_t> &goffs,
-                       unsigned char *base, std::vector<pentadsolver_grid_t> &out) {
+                       unsigned char *base, std::vector<pentadsolver_grid_t> &out,
+                       bool on_q = false) {
   out.resize(count);
   for (int i = 0; i < count; ++i) {
     const size_t N = (size_t)shapes[i].L.n * (size_t)shapes[i].L.n_sys;
@@ -1095,7 +1113,9 @@ void refine_fp32_grids(int count, const pentadsolver_grid_t *grids,
     out[i] = grids[i];
     out[i].ds = s; out[i].dl = s + N; out[i].d = s + 2 * N; out[i].du = s + 3 * N;
     out[i].dw = s + 4 * N;
-    out[i].x = r;
+    out[i].x = on_q ? reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(r) +
+                                                round256(N * sizeof(float)))
+                    : r;
   }
 }
 
@@ -1632,6 +1652,17 @@ extern "C" pentadStatus_t pentadsolver_plan_execute(pentadsolver_plan_t plan, vo
     return penta::launch_refine_step(k, none, p.rtable, p.count, p.chunks, s) == cudaSuccess;
   };
   pentadStatus_t st;
+  if (p.steps <= 1) {  // the one-step form: no FP64 copies of x0 and b
+    if (!step(penta::RefineStep::FirstCast)) return PENTAD_STATUS_EXECUTION_FAILED;
+    if ((st = penta::plan_run<float>(*p.fp32, s)) != PENTAD_STATUS_SUCCESS) return st;
+    if (p.steps == 0)
+      return step(penta::RefineStep::Lift) ? PENTAD_STATUS_SUCCESS
+                                           : PENTAD_STATUS_EXECUTION_FAILED;
+    if (!step(penta::RefineStep::Residual1)) return PENTAD_STATUS_EXECUTION_FAILED;
+    if ((st = penta::plan_run<float>(*p.fp32q, s)) != PENTAD_STATUS_SUCCESS) return st;
+    return step(penta::RefineStep::Correct1) ? PENTAD_STATUS_SUCCESS
+                                             : PENTAD_STATUS_EXECUTION_FAILED;
+  }
   if (!step(penta::RefineStep::PrepareCast)) return PENTAD_STATUS_EXECUTION_FAILED;
   if ((st = penta::plan_run<float>(*p.fp32, s)) != PENTAD_STATUS_SUCCESS) return st;
   if (!step(penta::RefineStep::Lift)) return PENTAD_STATUS_EXECUTION_FAILED;
@@ -1710,10 +1741,11 @@ extern "C" pentadStatus_t pentadsolver_refine_plan_buffer_size(pentadsolver_hand
   std::vector<pentadsolver_grid_t> g32;
   penta::refine_fp32_grids(count, grids, shapes, goffs,
                            reinterpret_cast<unsigned char *>(uintptr_t(256)), g32);
-  size_t plan_bytes = 0;
-  st = pentadsolver_plan_buffer_size(h, 4, count, g32.data(), solvedim, &plan_bytes);
+  // two job tables (over r, and over q for the one-step form), one scratch
+  size_t tb = 0, sb = 0;
+  st = pentadsolver_plan_sizes(h, 4, count, g32.data(), solvedim, &tb, &sb);
   if (st != PENTAD_STATUS_SUCCESS) return st;
-  *bytes = fp32_off + plan_bytes;
+  *bytes = fp32_off + 2 * penta::round256(tb) + sb;
   return PENTAD_STATUS_SUCCESS;
 }
 
@@ -1755,10 +1787,26 @@ extern "C" pentadStatus_t pentadsolver_refine_plan_create(pentadsolver_handle_t 
     penta::TuneChoice tc;
     if (ctas == 0 && penta::tune_lookup(rkey, tc) && tc.ctas > 0) ctas = tc.ctas;
   }
+  const size_t tb2 = 2 * penta::round256(tb);
   st = penta::plan_build<float>(*ctx, count, g32.data(), solvedim, base + fp32_off, tb,
-                                base + fp32_off + tb, buffer_bytes - fp32_off - tb, ctas, fp32,
+                                base + fp32_off + tb2, buffer_bytes - fp32_off - tb2, ctas, fp32,
                                 &why);
   if (st != PENTAD_STATUS_SUCCESS) return st;
+  penta::Plan *fp32q = nullptr;
+  if (steps == 1) {  // the second sweep of the one-step form solves q in place
+    std::vector<pentadsolver_grid_t> g32q;
+    penta::refine_fp32_grids(count, grids, shapes, goffs, base, g32q, true);
+    st = penta::plan_build<float>(*ctx, count, g32q.data(), solvedim,
+                                  base + fp32_off + penta::round256(tb), tb, base + fp32_off + tb2,
+                                  buffer_bytes - fp32_off - tb2, ctas, fp32q, &why);
+    if (st != PENTAD_STATUS_SUCCESS) {
+      delete fp32;
+      return st;
+    }
+    penta::status_slot_release(fp32q->slot, ctx->device);  // report with the first sweep
+    fp32q->slot = fp32->slot;
+    fp32q->owns_slot = false;
+  }
   // the grid table of the FP64 steps
   std::vector<penta::RefineGrid> table(count);
   double *est = reinterpret_cast<double *>(base + penta::round256(count * sizeof(penta::RefineGrid)));
@@ -1782,6 +1830,7 @@ extern "C" pentadStatus_t pentadsolver_refine_plan_create(pentadsolver_handle_t 
   if (penta::copy_h2d(*ctx, base, table.data(), count * sizeof(penta::RefineGrid)) !=
       cudaSuccess) {
     cudaGetLastError();
+    delete fp32q;
     delete fp32;
     return PENTAD_STATUS_EXECUTION_FAILED;
   }
@@ -1796,6 +1845,7 @@ extern "C" pentadStatus_t pentadsolver_refine_plan_create(pentadsolver_handle_t 
   p->est = est;
   p->count = count;
   p->fp32 = fp32;
+  p->fp32q = fp32q;
   p->tkey = rkey;
   p->desc = "refine steps=" + std::to_string(steps) + " over " + fp32->desc;
   *plan = new pentadsolver_plan_s{p};
@@ -1947,6 +1997,7 @@ extern "C" pentadStatus_t pentadsolver_autotune_plan(pentadsolver_plan_t plan, i
   pentadStatus_t st = PENTAD_STATUS_SUCCESS;
   for (double f : kFractions) {
     launching.ctas = std::max(1, (int)(ctx.sm_count * f));
+    if (p.fp32q) p.fp32q->ctas = launching.ctas;
     if ((st = pentadsolver_plan_execute(plan, stream)) != PENTAD_STATUS_SUCCESS) break;  // warm-up
     bool ok = cudaEventRecord(e0, static_cast<cudaStream_t>(stream)) == cudaSuccess;
     for (int r = 0; ok && r < reps; ++r) ok = pentadsolver_plan_execute(plan, stream) == PENTAD_STATUS_SUCCESS;
@@ -1967,6 +2018,7 @@ extern "C" pentadStatus_t pentadsolver_autotune_plan(pentadsolver_plan_t plan, i
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   launching.ctas = st == PENTAD_STATUS_SUCCESS ? best : before;
+  if (p.fp32q) p.fp32q->ctas = launching.ctas;
   if (st != PENTAD_STATUS_SUCCESS) return st;
   penta::TuneChoice c;
   c.ctas = best;

@@ -147,13 +147,20 @@ struct RefineGrid {
   double *b;                            // the saved right-hand side
   float *s_ds, *s_dl, *s_d, *s_du, *s_dw;  // FP32 coefficient copies
   float *r;                             // FP32 right-hand side / correction
+  float *q;                             // FP32 residual / correction of a one-step solve
   double *est;                          // [max|last correction|, max|x|]
   long long n_points;
   int n, inner;                         // line length, row stride
   int chunk_base;                       // first CTA of this grid in a table launch
   int pad_;
 };
-enum class RefineStep { PrepareCast, Prepare, Lift, Residual, Correct };
+enum class RefineStep {
+  PrepareCast, Prepare, Lift, Residual, Correct,
+  // one refinement step without an FP64 copy of the first iterate or of b:
+  // r = fl32(x) (b stays in x), the sweep leaves x0 in r, q = fl32(x - A x0),
+  // the sweep leaves d in q, x = x0 + d
+  FirstCast, First, Residual1, Correct1
+};
 int refine_chunks(long long n_points);
 cudaError_t launch_refine_step(RefineStep step, const RefineGrid &one, const RefineGrid *table,
                                int count, int total_chunks, cudaStream_t stream);

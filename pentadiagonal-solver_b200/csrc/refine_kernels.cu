@@ -7,7 +7,12 @@
 //             d = solve32(A32, r)                     (FP32 sweep)
 //             x = x + d                               (FP64 correction)
 // The residual and the correction are the only FP64 arithmetic; the sweeps
-// are the library's FP32 kernels.  Each kernel here walks the points of one
+// are the library's FP32 kernels.  With one refinement step (or none) the
+// first iterate stays in FP32 (x0 in r) and b stays in the caller's x until
+// the correction writes the result: q = fl32(b - A x0) goes to a second FP32
+// array, the second sweep solves it in place, and x = x0 + d -- the same
+// values as the general form without its FP64 copies of x0 and b (140
+// instead of 168 bytes per point with cached FP32 coefficients).  Each kernel here walks the points of one
 // or many grids (a grid table; one CTA handles a chunk of one grid), so a
 // batch of uneven grids is one launch per step.
 //
@@ -46,7 +51,7 @@ __device__ __forceinline__ const RefineGrid &grid_of(const RefineGrid &one,
 }
 
 __global__ void __launch_bounds__(kThreads)
-rf_prepare_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__restrict__ table, int count, int cast_coefficients) {
+rf_prepare_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__restrict__ table, int count, int cast_coefficients, int save_b) {
   long long first;
   const RefineGrid &g = grid_of(one, table, count, blockIdx.x, first);
   const long long end = min(first + kChunk, g.n_points);
@@ -59,7 +64,7 @@ rf_prepare_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__re
       g.s_dw[i] = (float)g.dw[i];
     }
     const double b = g.x[i];
-    g.b[i] = b;
+    if (save_b) g.b[i] = b;
     g.r[i] = (float)b;
   }
 }
@@ -92,6 +97,26 @@ rf_residual_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__r
   }
 }
 
+// q = fl32(b - A x0) with b still in the caller's x and x0 the FP32 iterate in
+// r, FP64 arithmetic: the same values as Lift followed by Residual.
+__global__ void __launch_bounds__(kThreads)
+rf_residual1_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__restrict__ table, int count) {
+  long long first;
+  const RefineGrid &g = grid_of(one, table, count, blockIdx.x, first);
+  const long long end = min(first + kChunk, g.n_points);
+  const long long s = g.inner;
+  const int n = g.n;
+  for (long long i = first + threadIdx.x; i < end; i += kThreads) {
+    const int k = (int)((i / s) % n);  // row within its line
+    double ax = g.d[i] * (double)g.r[i];
+    if (k >= 2) ax = fma(g.ds[i], (double)g.r[i - 2 * s], ax);
+    if (k >= 1) ax = fma(g.dl[i], (double)g.r[i - s], ax);
+    if (k <= n - 2) ax = fma(g.du[i], (double)g.r[i + s], ax);
+    if (k <= n - 3) ax = fma(g.dw[i], (double)g.r[i + 2 * s], ax);
+    g.q[i] = (float)(g.x[i] - ax);
+  }
+}
+
 __device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
   // non-negative doubles order like their bit patterns
   atomicMax(reinterpret_cast<unsigned long long *>(addr),
@@ -108,6 +133,30 @@ rf_correct_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__re
   for (long long i = first + threadIdx.x; i < end; i += kThreads) {
     const double dd = (double)g.r[i];
     const double xn = g.x[i] + dd;
+    g.x[i] = xn;
+    md = fmax(md, fabs(dd));
+    mx = fmax(mx, fabs(xn));
+  }
+  for (int o = 16; o > 0; o /= 2) {
+    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_nonneg(&g.est[0], md);
+    atomic_max_nonneg(&g.est[1], mx);
+  }
+}
+
+// x = fl64(x0) + fl64(d) with x0 in r and d in q; est as rf_correct_kernel.
+__global__ void __launch_bounds__(kThreads)
+rf_correct1_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__restrict__ table, int count) {
+  long long first;
+  const RefineGrid &g = grid_of(one, table, count, blockIdx.x, first);
+  const long long end = min(first + kChunk, g.n_points);
+  double md = 0.0, mx = 0.0;
+  for (long long i = first + threadIdx.x; i < end; i += kThreads) {
+    const double dd = (double)g.q[i];
+    const double xn = (double)g.r[i] + dd;
     g.x[i] = xn;
     md = fmax(md, fabs(dd));
     mx = fmax(mx, fabs(xn));
@@ -142,12 +191,26 @@ cudaError_t launch_refine_step(RefineStep step, const RefineGrid &one, const Ref
   if (total_chunks <= 0) return cudaSuccess;
   switch (step) {
     case RefineStep::PrepareCast:
-      rf_prepare_kernel<<<total_chunks, kThreads, 0, stream>>>(one, table, count, 1);
+      rf_prepare_kernel<<<total_chunks, kThreads, 0, stream>>>(one, table, count, 1, 1);
       break;
     case RefineStep::Prepare:
-      rf_prepare_kernel<<<total_chunks, kThreads, 0, stream>>>(one, table, count, 0);
+      rf_prepare_kernel<<<total_chunks, kThreads, 0, stream>>>(one, table, count, 0, 1);
       break;
-    case RefineStep::Lift:
+    case RefineStep::FirstCast:
+      rf_prepare_kernel<<<total_chunks, kThreads, 0, stream>>>(one, table, count, 1, 0);
+      break;
+    case RefineStep::First:
+      rf_prepare_kernel<<<total_chunks, kThreads, 0, stream>>>(one, table, count, 0, 0);
+      break;
+    case RefineStep::Residual1:
+      rf_residual1_kernel<<<total_chunks, kThreads, 0, stream>>>(one, table, count);
+      break;
+    case RefineStep::Correct1:
+      rf_clear_kernel<<<(count + 127) / 128, 128, 0, stream>>>(one, table, count);
+      rf_correct1_kernel<<<total_chunks, kThreads, 0, stream>>>(one, table, count);
+      break;
+    case RefineStep::Lift:  // no correction yet: the estimate reads zero
+      rf_clear_kernel<<<(count + 127) / 128, 128, 0, stream>>>(one, table, count);
       rf_lift_kernel<<<total_chunks, kThreads, 0, stream>>>(one, table, count);
       break;
     case RefineStep::Residual:
