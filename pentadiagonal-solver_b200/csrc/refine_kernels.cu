@@ -123,6 +123,30 @@ __device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
             (unsigned long long)__double_as_longlong(v));
 }
 
+// est = max(est, (md, mx)) for the whole CTA: one warp-level and one
+// CTA-level reduction, then at most two atomics, skipped when the stored
+// maxima are already at least as large (a stale read of them only costs an
+// atomic: the maxima never decrease).  Every thread of the CTA calls it.
+__device__ __forceinline__ void cta_max_into(double *est, double md, double mx) {
+  __shared__ double part[2][kThreads / 32];
+  for (int o = 16; o > 0; o /= 2) {
+    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  const int w = threadIdx.x / 32;
+  if ((threadIdx.x & 31) == 0) {
+    part[0][w] = md;
+    part[1][w] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    double v = part[threadIdx.x][0];
+    for (int k = 1; k < kThreads / 32; ++k) v = fmax(v, part[threadIdx.x][k]);
+    double *const slot = est + threadIdx.x;
+    if (v > *reinterpret_cast<volatile double *>(slot)) atomic_max_nonneg(slot, v);
+  }
+}
+
 // x += fl64(d); est = (max|d|, max|x|) over the grid.
 __global__ void __launch_bounds__(kThreads)
 rf_correct_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__restrict__ table, int count) {
@@ -137,14 +161,7 @@ rf_correct_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__re
     md = fmax(md, fabs(dd));
     mx = fmax(mx, fabs(xn));
   }
-  for (int o = 16; o > 0; o /= 2) {
-    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
-    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomic_max_nonneg(&g.est[0], md);
-    atomic_max_nonneg(&g.est[1], mx);
-  }
+  cta_max_into(g.est, md, mx);
 }
 
 // x = fl64(x0) + fl64(d) with x0 in r and d in q; est as rf_correct_kernel.
@@ -161,14 +178,7 @@ rf_correct1_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__r
     md = fmax(md, fabs(dd));
     mx = fmax(mx, fabs(xn));
   }
-  for (int o = 16; o > 0; o /= 2) {
-    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
-    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomic_max_nonneg(&g.est[0], md);
-    atomic_max_nonneg(&g.est[1], mx);
-  }
+  cta_max_into(g.est, md, mx);
 }
 
 // Clear the estimate before a correction step.
