@@ -12,6 +12,8 @@
            the three captured in one CUDA graph; FP64 and FP32 + 1 refinement
            step (all 96 grids); against per-grid single calls.  Forward errors
            of both forms against the CPU oracle, grid by grid.
+  refine1  one-step refined solves of config 2's 512^3 grid, 3 timed calls per axis
+           (FP32 coefficient copies cached): the launch-list command.
   3split   config 3's FP64 plans per axis and bucket of line length along it (32-64
            ... 321-384, and all): where the time goes.
   config4  serving: a Poisson stream (2000 requests/s) of grids with per-axis
@@ -57,7 +59,7 @@ bench.py, this script uses oracle/ only as the checker (forward errors) and
 for the reference's own CPU code timed as the baseline; the solves and grids
 it measures are the library's.
 
-  python bench_configs.py [--configs 0,2,3,3split,4,odd,mesh,refapp]
+  python bench_configs.py [--configs 0,2,refine1,3,3split,4,odd,mesh,refapp]
 """
 from __future__ import annotations
 
@@ -433,6 +435,29 @@ def config3_split(n_grids=96, lo=32, hi=384, seed=33):
     return out
 
 
+def config_refine1(n=512, calls=3):
+    """One-step refined solves of config 2's grid (FP32 coefficient copies
+    cached after the first call), `calls` timed calls per axis: the command
+    whose kernel launch list shows where the refined form's time goes."""
+    import pentadsolver as ps
+
+    dims = (n, n, n)
+    p = dev_problem(dims, 2)
+    out = {"config": "refine1_512cube", "points": n ** 3, "axes": []}
+    for axis in range(3):
+        buf = ps.alloc_refine_buffer(list(dims), axis)
+        args = (p["ds"], p["dl"], p["d"], p["du"], p["dw"], p["x"], axis)
+        ps.gpsv_batch_refine(*args, steps=1, buffer=buf)
+        ms = timed(lambda: ps.gpsv_batch_refine(*args, steps=1, buffer=buf,
+                                                reuse_fp32_coefficients=True),
+                   reps=calls, warmup=0)
+        out["axes"].append({"axis": axis, "ms": round(ms, 4),
+                            "GBps_equiv": round(56 * n ** 3 / ms / 1e6, 1)})
+        del buf
+    out["peak_GBps"] = peak()
+    return out
+
+
 def config_odd(reps=10):
     import os
 
@@ -617,10 +642,10 @@ def main():
     runs = {"0": config0, "2": lambda: config2(args.n2), "3": lambda: config3(args.grids3),
             "4": lambda: config4(seconds=args.seconds4), "mesh": config_mesh,
             "refapp": config_refapp, "odd": lambda: config_odd(args.odd_reps),
-            "3split": config3_split}
+            "3split": config3_split, "refine1": config_refine1}
     from bench import ClockSampler
 
-    for c in ("0", "2", "3", "3split", "4", "odd", "mesh", "refapp"):
+    for c in ("0", "2", "refine1", "3", "3split", "4", "odd", "mesh", "refapp"):
         if c in want:
             t0 = time.time()
             with ClockSampler(0) as clk:

@@ -50,11 +50,26 @@ __device__ __forceinline__ const RefineGrid &grid_of(const RefineGrid &one,
   return table[lo];
 }
 
+// Whether points [first, end) of an array can be walked in pairs: an even
+// start and end, and an array aligned for the pair's width.
+__device__ __forceinline__ bool pairs_ok(long long first, long long end, const void *a,
+                                         int width) {
+  return ((first | end) & 1) == 0 && (reinterpret_cast<uintptr_t>(a) & (width - 1)) == 0;
+}
+
 __global__ void __launch_bounds__(kThreads)
 rf_prepare_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__restrict__ table, int count, int cast_coefficients, int save_b) {
   long long first;
   const RefineGrid &g = grid_of(one, table, count, blockIdx.x, first);
   const long long end = min(first + kChunk, g.n_points);
+  if (!cast_coefficients && !save_b && pairs_ok(first, end, g.x, 16) &&
+      pairs_ok(first, end, g.r, 8)) {  // the one-step form's steady state: pairs
+    for (long long i = first + 2 * threadIdx.x; i < end; i += 2 * kThreads) {
+      const double2 b = *reinterpret_cast<const double2 *>(g.x + i);
+      *reinterpret_cast<float2 *>(g.r + i) = make_float2((float)b.x, (float)b.y);
+    }
+    return;
+  }
   for (long long i = first + threadIdx.x; i < end; i += kThreads) {
     if (cast_coefficients) {
       g.s_ds[i] = (float)g.ds[i];
@@ -171,12 +186,25 @@ rf_correct1_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__r
   const RefineGrid &g = grid_of(one, table, count, blockIdx.x, first);
   const long long end = min(first + kChunk, g.n_points);
   double md = 0.0, mx = 0.0;
-  for (long long i = first + threadIdx.x; i < end; i += kThreads) {
-    const double dd = (double)g.q[i];
-    const double xn = (double)g.r[i] + dd;
-    g.x[i] = xn;
-    md = fmax(md, fabs(dd));
-    mx = fmax(mx, fabs(xn));
+  if (pairs_ok(first, end, g.x, 16) && pairs_ok(first, end, g.r, 8) &&
+      pairs_ok(first, end, g.q, 8)) {
+    for (long long i = first + 2 * threadIdx.x; i < end; i += 2 * kThreads) {
+      const float2 d2 = *reinterpret_cast<const float2 *>(g.q + i);
+      const float2 x2 = *reinterpret_cast<const float2 *>(g.r + i);
+      const double d0 = (double)d2.x, d1 = (double)d2.y;
+      const double2 xn = make_double2((double)x2.x + d0, (double)x2.y + d1);
+      *reinterpret_cast<double2 *>(g.x + i) = xn;
+      md = fmax(md, fmax(fabs(d0), fabs(d1)));
+      mx = fmax(mx, fmax(fabs(xn.x), fabs(xn.y)));
+    }
+  } else {
+    for (long long i = first + threadIdx.x; i < end; i += kThreads) {
+      const double dd = (double)g.q[i];
+      const double xn = (double)g.r[i] + dd;
+      g.x[i] = xn;
+      md = fmax(md, fabs(dd));
+      mx = fmax(mx, fabs(xn));
+    }
   }
   cta_max_into(g.est, md, mx);
 }

@@ -136,6 +136,31 @@ def test_refine_reuses_fp32_coefficients(cuda, steps):
     assert fwd_err(first.cpu().numpy(), ref) <= 1e-10
 
 
+def test_refine_one_step_same_bits_on_unaligned_arrays(cuda):
+    # arrays one element past a 16-byte boundary take the element-wise FP64
+    # steps one point at a time instead of in pairs: the same bits
+    import torch
+
+    dims = (37, 30, 22)
+    co = fixtures.random_dominant(dims, 13, np.float64)
+    n = int(np.prod(dims))
+    results = []
+    for shift in (0, 1):
+        dv = {}
+        for k in NAMES:
+            raw = torch.empty(n + 2, dtype=torch.float64, device="cuda")
+            dv[k] = raw[shift:shift + n].view(*reversed(dims))
+            dv[k].copy_(torch.from_numpy(co[k]))
+        assert (dv["x"].data_ptr() % 16 == 0) == (shift == 0)
+        buf = ps.alloc_refine_buffer(list(dims), 0)
+        ps.gpsv_batch_refine(*(dv[k] for k in NAMES), 0, steps=1, buffer=buf)
+        results.append((dv["x"].clone(), ps.refine_estimate(buf)))
+    assert torch.equal(results[0][0], results[1][0])
+    assert results[0][1] == results[1][1]
+    ref = oracle_solution(co, 0)
+    assert fwd_err(results[0][0].cpu().numpy(), ref) <= 1e-10
+
+
 def test_refine_estimate_reads_zero_without_a_step(cuda):
     # the estimate slot of a buffer that held anything reads (0, 0) after a
     # solve without refinement steps
