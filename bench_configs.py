@@ -10,7 +10,9 @@
   config3  96 grids, N_x, N_y, N_z ~ U[32, 384] (seeded), random dominant
            coefficients, x, y and z each one plan (one persistent launch),
            the three captured in one CUDA graph; FP64 and FP32 + 1 refinement
-           step (all 96 grids); against per-grid single calls.  Forward errors
+           step (all 96 grids; casting the coefficients to FP32 in every execute,
+           and keeping the copies of an earlier execute); against per-grid
+           single calls.  Forward errors
            of both forms against the CPU oracle, grid by grid.
   refine1  one-step refined solves of config 2's 512^3 grid, 3 timed calls per axis
            (FP32 coefficient copies cached): the launch-list command.
@@ -322,7 +324,7 @@ def config3(n_grids=96, lo=32, hi=384, seed=33):
     try:
         for g, r in zip(sub, sub_rhs):
             g["x"].copy_(r)
-        ms_axes = []
+        ms_axes, ms_reuse = [], []
         out["tuned_ctas_ir1"] = []
         for axis in range(3):
             out["tuned_ctas_ir1"].append(tuner.tune_plan(sub, axis, refine_steps=1)["best"]["ctas"])
@@ -338,6 +340,13 @@ def config3(n_grids=96, lo=32, hi=384, seed=33):
             with torch.cuda.graph(graph, stream=s):
                 rp.execute(s)
             ms_axes.append(timed(lambda: (put_back(), graph.replay())) - timed(put_back))
+            # the same with the FP32 copies kept from the executes above (fixed
+            # coefficients, as in an ADI loop)
+            graph_r = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph_r, stream=s):
+                rp.execute(s, reuse_fp32=True)
+            ms_reuse.append(timed(lambda: (put_back(), graph_r.replay())) - timed(put_back))
+            del graph_r
             put_back()
             graph.replay()           # leave this axis solved, then the next axis
             torch.cuda.synchronize()
@@ -348,6 +357,8 @@ def config3(n_grids=96, lo=32, hi=384, seed=33):
         ms_r = sum(ms_axes)
         out["ir1_ms_xyz"] = round(ms_r, 3)
         out["ir1_ms_per_axis"] = [round(v, 3) for v in ms_axes]
+        out["ir1_cached_fp32_ms_xyz"] = round(sum(ms_reuse), 3)
+        out["ir1_cached_fp32_ms_per_axis"] = [round(v, 3) for v in ms_reuse]
         out["ir1_GBps_equiv"] = round(3 * 56 * pts_ir / (ms_r * 1e-3) / 1e9, 1)
         out["ir1_fwd_err_max_vs_oracle"] = oracle_errors(sub, sub_rhs,
                                                          [g["x"] for g in sub], axes=(0, 1, 2))

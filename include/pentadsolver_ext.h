@@ -125,6 +125,16 @@ EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_create_split(
     int ctas, pentadsolver_plan_t *plan);
 EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_execute(pentadsolver_plan_t plan,
                                                               void *stream);
+/* As pentadsolver_plan_execute.  With PENTADSOLVER_PLAN_REUSE_FP32 in `flags`
+ * a refinement plan keeps the FP32 copies of the coefficients that an earlier
+ * execute of this plan made, instead of casting them again: the caller
+ * vouches that the grids' coefficients have not changed since (an ADI loop's
+ * fixed coefficients).  The first execute, and any after one whose cast
+ * did not launch, casts anyway.  Ignored by plans without refinement; other bits are invalid.
+ * In a captured execute the choice is made at capture. */
+#define PENTADSOLVER_PLAN_REUSE_FP32 1
+EXTERN_C PENTAD_API pentadStatus_t pentadsolver_plan_execute_ex(pentadsolver_plan_t plan,
+                                                                 void *stream, int flags);
 EXTERN_C PENTAD_API const char *pentadsolver_plan_describe(pentadsolver_plan_t plan);
 /* Times `reps` executes of the plan with each of several CTA counts (all SMs,
  * 90%, 75%, 50%), keeps the fastest for this plan and records it in the

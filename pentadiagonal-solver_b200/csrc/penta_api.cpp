@@ -744,6 +744,7 @@ struct Plan {
   int count = 0;
   Plan *fp32 = nullptr;          // the FP32 plan over the cast copies
   Plan *fp32q = nullptr;         // the same over the q arrays (one-step form)
+  bool cast_done = false;        // the FP32 copies hold the coefficients of an execute
   bool owns_slot = true;         // false: fp32q reports into fp32's slot
   // the slot the plan's kernels report into (a refine plan's FP32 sweeps)
   int report_slot() const { return fp32 ? fp32->slot : slot; }
@@ -1639,8 +1640,10 @@ extern "C" pentadStatus_t pentadsolver_plan_create_split(
   return PENTAD_STATUS_SUCCESS;
 }
 
-extern "C" pentadStatus_t pentadsolver_plan_execute(pentadsolver_plan_t plan, void *stream) {
-  if (plan == nullptr || plan->p == nullptr) return PENTAD_STATUS_INVALID_VALUE;
+extern "C" pentadStatus_t pentadsolver_plan_execute_ex(pentadsolver_plan_t plan, void *stream,
+                                                     int flags) {
+  if (plan == nullptr || plan->p == nullptr || (flags & ~PENTADSOLVER_PLAN_REUSE_FP32) != 0)
+    return PENTAD_STATUS_INVALID_VALUE;
   penta::Plan &p = *plan->p;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (!p.refine)
@@ -1652,8 +1655,14 @@ extern "C" pentadStatus_t pentadsolver_plan_execute(pentadsolver_plan_t plan, vo
     return penta::launch_refine_step(k, none, p.rtable, p.count, p.chunks, s) == cudaSuccess;
   };
   pentadStatus_t st;
+  // the FP32 copies are cast again unless the caller vouches that the
+  // coefficients did not change since an execute that cast them
+  const bool cast = !(p.cast_done && (flags & PENTADSOLVER_PLAN_REUSE_FP32));
+  p.cast_done = false;  // set again once this execute's cast is queued
   if (p.steps <= 1) {  // the one-step form: no FP64 copies of x0 and b
-    if (!step(penta::RefineStep::FirstCast)) return PENTAD_STATUS_EXECUTION_FAILED;
+    if (!step(cast ? penta::RefineStep::FirstCast : penta::RefineStep::First))
+      return PENTAD_STATUS_EXECUTION_FAILED;
+    p.cast_done = true;
     if ((st = penta::plan_run<float>(*p.fp32, s)) != PENTAD_STATUS_SUCCESS) return st;
     if (p.steps == 0)
       return step(penta::RefineStep::Lift) ? PENTAD_STATUS_SUCCESS
@@ -1663,7 +1672,9 @@ extern "C" pentadStatus_t pentadsolver_plan_execute(pentadsolver_plan_t plan, vo
     return step(penta::RefineStep::Correct1) ? PENTAD_STATUS_SUCCESS
                                              : PENTAD_STATUS_EXECUTION_FAILED;
   }
-  if (!step(penta::RefineStep::PrepareCast)) return PENTAD_STATUS_EXECUTION_FAILED;
+  if (!step(cast ? penta::RefineStep::PrepareCast : penta::RefineStep::Prepare))
+    return PENTAD_STATUS_EXECUTION_FAILED;
+  p.cast_done = true;
   if ((st = penta::plan_run<float>(*p.fp32, s)) != PENTAD_STATUS_SUCCESS) return st;
   if (!step(penta::RefineStep::Lift)) return PENTAD_STATUS_EXECUTION_FAILED;
   for (int k = 0; k < p.steps; ++k) {
@@ -1672,6 +1683,10 @@ extern "C" pentadStatus_t pentadsolver_plan_execute(pentadsolver_plan_t plan, vo
     if (!step(penta::RefineStep::Correct)) return PENTAD_STATUS_EXECUTION_FAILED;
   }
   return PENTAD_STATUS_SUCCESS;
+}
+
+extern "C" pentadStatus_t pentadsolver_plan_execute(pentadsolver_plan_t plan, void *stream) {
+  return pentadsolver_plan_execute_ex(plan, stream, 0);
 }
 
 extern "C" const char *pentadsolver_plan_describe(pentadsolver_plan_t plan) {

@@ -377,9 +377,12 @@ class Plan:
         if st != SUCCESS:
             raise PentadError(st, "plan create")
 
-    def execute(self, stream=None) -> None:
-        st = _typed("pentadsolver_plan_execute", [_P, _P])(
-            self._plan, _stream_ptr(stream, self.device))
+    def execute(self, stream=None, reuse_fp32: bool = False) -> None:
+        """Run the plan.  ``reuse_fp32`` (refinement plans): keep the FP32
+        coefficient copies of an earlier execute -- the caller vouches that
+        the coefficients have not changed (``PENTADSOLVER_PLAN_REUSE_FP32``)."""
+        st = _typed("pentadsolver_plan_execute_ex", [_P, _P, _I])(
+            self._plan, _stream_ptr(stream, self.device), 1 if reuse_fp32 else 0)
         if st != SUCCESS:
             raise PentadError(st, "plan execute")
 

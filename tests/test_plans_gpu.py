@@ -161,6 +161,30 @@ def test_refine_one_step_same_bits_on_unaligned_arrays(cuda):
     assert fwd_err(results[0][0].cpu().numpy(), ref) <= 1e-10
 
 
+@pytest.mark.parametrize("steps", [1, 2])
+def test_refine_plan_reuses_its_fp32_copies(cuda, steps):
+    # an execute that keeps the FP32 copies of an earlier execute gives the same
+    # bits as one that casts again; the first execute casts even when asked to
+    # reuse
+    import torch
+
+    dims_list = [(33, 20, 17), (48, 24, 12)]
+    probs = [fixtures.random_dominant(d, 70 + i, np.float64) for i, d in enumerate(dims_list)]
+    devs = [to_dev(co) for co in probs]
+    rhs = [dv["x"].clone() for dv in devs]
+    with ps.Plan(devs, 1, refine_steps=steps) as plan:
+        plan.execute(reuse_fp32=True)
+        first = [dv["x"].clone() for dv in devs]
+        for dv, r in zip(devs, rhs):
+            dv["x"].copy_(r)
+        plan.execute(reuse_fp32=True)
+        again = [dv["x"].clone() for dv in devs]
+        assert plan.status_check() == (ps.SUCCESS, 0)
+    for a, b, co in zip(first, again, probs):
+        assert torch.equal(a, b)
+        assert fwd_err(a.cpu().numpy(), oracle_solution(co, 1)) <= 1e-10
+
+
 def test_refine_estimate_reads_zero_without_a_step(cuda):
     # the estimate slot of a buffer that held anything reads (0, 0) after a
     # solve without refinement steps
