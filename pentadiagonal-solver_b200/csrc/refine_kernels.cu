@@ -57,16 +57,36 @@ __device__ __forceinline__ bool pairs_ok(long long first, long long end, const v
   return ((first | end) & 1) == 0 && (reinterpret_cast<uintptr_t>(a) & (width - 1)) == 0;
 }
 
+__device__ __forceinline__ void cast_pair(const double *src, float *dst, long long i) {
+  const double2 v = *reinterpret_cast<const double2 *>(src + i);
+  *reinterpret_cast<float2 *>(dst + i) = make_float2((float)v.x, (float)v.y);
+}
+
+__device__ __forceinline__ bool cast_pairs_ok(const RefineGrid &g, long long first,
+                                              long long end) {
+  return pairs_ok(first, end, g.ds, 16) && pairs_ok(first, end, g.dl, 16) &&
+         pairs_ok(first, end, g.d, 16) && pairs_ok(first, end, g.du, 16) &&
+         pairs_ok(first, end, g.dw, 16) && pairs_ok(first, end, g.s_ds, 8) &&
+         pairs_ok(first, end, g.s_dl, 8) && pairs_ok(first, end, g.s_d, 8) &&
+         pairs_ok(first, end, g.s_du, 8) && pairs_ok(first, end, g.s_dw, 8);
+}
+
 __global__ void __launch_bounds__(kThreads)
 rf_prepare_kernel(const __grid_constant__ RefineGrid one, const RefineGrid *__restrict__ table, int count, int cast_coefficients, int save_b) {
   long long first;
   const RefineGrid &g = grid_of(one, table, count, blockIdx.x, first);
   const long long end = min(first + kChunk, g.n_points);
-  if (!cast_coefficients && !save_b && pairs_ok(first, end, g.x, 16) &&
-      pairs_ok(first, end, g.r, 8)) {  // the one-step form's steady state: pairs
+  if (!save_b && pairs_ok(first, end, g.x, 16) && pairs_ok(first, end, g.r, 8) &&
+      (!cast_coefficients || cast_pairs_ok(g, first, end))) {  // the one-step form: pairs
     for (long long i = first + 2 * threadIdx.x; i < end; i += 2 * kThreads) {
-      const double2 b = *reinterpret_cast<const double2 *>(g.x + i);
-      *reinterpret_cast<float2 *>(g.r + i) = make_float2((float)b.x, (float)b.y);
+      if (cast_coefficients) {
+        cast_pair(g.ds, g.s_ds, i);
+        cast_pair(g.dl, g.s_dl, i);
+        cast_pair(g.d, g.s_d, i);
+        cast_pair(g.du, g.s_du, i);
+        cast_pair(g.dw, g.s_dw, i);
+      }
+      cast_pair(g.x, g.r, i);
     }
     return;
   }
