@@ -143,6 +143,15 @@ __device__ __forceinline__ void tma_load_2d_hint(void *dst, const CUtensorMap *m
       "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar)), "l"(pol)
       : "memory");
 }
+// Bring a tile of a 2-D tensor into L2 without a shared-memory destination.
+__device__ __forceinline__ void tma_prefetch_2d_hint(const CUtensorMap *map, int c0, int c1,
+                                                     uint64_t pol) {
+  asm volatile(
+      "cp.async.bulk.prefetch.tensor.2d.L2.global.tile.L2::cache_hint [%0, {%1, %2}], %3;\n" ::"l"(
+          reinterpret_cast<uint64_t>(map)),
+      "r"(c0), "r"(c1), "l"(pol)
+      : "memory");
+}
 __device__ __forceinline__ void tma_load_3d_hint(void *dst, const CUtensorMap *map, uint64_t *bar,
                                                  int c0, int c1, int c2, uint64_t pol) {
   asm volatile(

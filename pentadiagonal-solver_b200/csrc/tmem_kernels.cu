@@ -497,13 +497,21 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
             const bool lower = r_dn < n;  // else all rows are virtual: not loaded
             mbar_arrive_n(&full[slot], 31);  // for the lanes that copy nothing
             mbar_expect_tx(&full[slot], (lower ? 12u : 6u) * BOX * (unsigned)sizeof(F));
+            // along x an even stage and the next one read the two 64-byte
+            // halves of the same 128-byte line of every line (both tile
+            // halves): with flags bit 2 the next stage's tiles are requested
+            // into L2 now, so each line reaches DRAM as one burst
+            const bool pre = CONTIG && (flags & 4) && (g & 1) == 0 && g + 1 < n_stages;
 #pragma unroll
             for (int q = 0; q < 6; ++q) {
               if (CONTIG) {
                 tma_load_2d_hint(dst + (2 * q) * BOX, &J->maps[q], &full[slot], r_up, c0, pol_in);
+                if (pre) tma_prefetch_2d_hint(&J->maps[q], r_up + R, c0, pol_in);
                 if (lower)
                   tma_load_2d_hint(dst + (2 * q + 1) * BOX, &J->maps[kMirror[q]], &full[slot],
                                    r_dn, c0, pol_in);
+                if (pre && r_dn - R < n)
+                  tma_prefetch_2d_hint(&J->maps[kMirror[q]], r_dn - R, c0, pol_in);
               } else {
                 tma_load_3d_hint(dst + (2 * q) * BOX, &J->maps[q], &full[slot], c0, r_up, c2,
                                  pol_in);
@@ -1443,6 +1451,20 @@ int scratch_grid_cap(const SolveArgs<F> &a, const TmemConfig &c, long long tiles
   return cap >= sm_count ? sm_count : (cap < floor_ctas ? floor_ctas : (int)cap);
 }
 
+// flags bit 2: along x, an even stage prefetches the next stage's tiles into
+// L2.  It pays only where the launch caps its CTAs to keep the (dw2, x2)
+// scratch in L2 (FP64 512^3 along x: 1.61 against 1.65 ms); elsewhere it cost
+// 0.5-3.5% (256^3, FP32, and the batched launches of uneven grids).
+// PENTA_TMEM_XPREFETCH=0 turns it off, =1 on for every x launch (measurement).
+int x_prefetch_flag(bool contig, bool capped) {
+  static const int mode = [] {
+    const char *e = std::getenv("PENTA_TMEM_XPREFETCH");
+    return e == nullptr ? -1 : (e[0] == '0' ? 0 : 1);
+  }();
+  if (!contig || mode == 0) return 0;
+  return (mode == 1 || capped) ? 4 : 0;
+}
+
 template <typename F>
 cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count,
                         cudaStream_t stream) {
@@ -1452,6 +1474,7 @@ cudaError_t launch_tmem(const SolveArgs<F> &a, const TmemConfig &c, int sm_count
   if (c.loads == 1 && !J.bulk) return cudaErrorInvalidValue;  // bulk loads need aligned arrays
   int flags = ((reinterpret_cast<uintptr_t>(a.scratch) % 128 == 0) ? 1 : 0);
   const int capped = scratch_grid_cap<F>(a, c, J.n_tiles, sm_count);
+  flags |= x_prefetch_flag(c.contig, capped < sm_count);
   // streamed loads evict-first when the grid is capped, and for FP32 along x with
   // dw2 in the buffer (1024 x 128 x 128: 118 against 129 us with normal priority)
   if (capped < sm_count || (sizeof(F) == 4 && c.contig && c.fmode == 1)) flags |= 2;
@@ -1496,7 +1519,8 @@ cudaError_t launch_tmem_batch(const void *device_jobs, int n_jobs, int total_til
   const TmemJob<F> *jobs = static_cast<const TmemJob<F> *>(device_jobs);
   // the load policy of single-grid launches (launch_tmem) on an uncapped grid:
   // evict-first streamed loads for FP32 along x with dw2 in the buffer
-  const int flags = (discard ? 1 : 0) | ((sizeof(F) == 4 && contig && fmode == 1) ? 2 : 0);
+  const int flags = (discard ? 1 : 0) | ((sizeof(F) == 4 && contig && fmode == 1) ? 2 : 0) |
+                    x_prefetch_flag(contig, false);
   // the default variant of each (layout, factor mode, loads)
   const std::vector<TmemConfig> &all = tmem_configs<F>();
   for (const TmemConfig &c : all) {
