@@ -234,6 +234,21 @@ class ProblemPool:
             ds, dl, du, dw = u(-1, 1), u(-1, 1), u(-1, 1), u(-1, 1)
             d = ds.abs() + dl.abs() + du.abs() + dw.abs() + u(1, 2)
             self.items.append({"ds": ds, "dl": dl, "d": d, "du": du, "dw": dw, "b": u(-1, 1)})
+        self._free = [[] for _ in self.shapes]   # iterates of finished requests, per problem
+
+    def iterate(self, i):
+        """A copy of problem i's right-hand side to solve in place (queued on the
+        current stream), in an iterate buffer that a finished request gave back
+        when there is one: a server holds its iterate memory instead of asking
+        the allocator for every request."""
+        x = self._free[i].pop() if self._free[i] else self.items[i]["b"].new_empty(
+            self.items[i]["b"].shape)
+        x.copy_(self.items[i]["b"])
+        return x
+
+    def give_back(self, i, x) -> None:
+        """Return an iterate whose request's work has completed on the device."""
+        self._free[i].append(x)
 
     def points(self, i) -> int:
         return int(math.prod(self.shapes[i]))
@@ -262,6 +277,7 @@ class CudaExecutor:
         self.status = {}   # request id -> status bits of the batch that solved it
         self.t0 = time.perf_counter()
         self.handle = ps.Handle()
+        self._seq_buf = None   # the sequential baseline's one buffer, sized on first use
         # per solve direction: does the refined form beat plain FP64 here?
         self.calibration = self.measure_costs() if calibrate else None
 
@@ -329,15 +345,20 @@ class CudaExecutor:
         with torch.cuda.stream(s):
             for r in b.requests:
                 p = self.pool.items[r.problem]
-                x = p["b"].clone()
+                x = self.pool.iterate(r.problem)
                 grids.append({"ds": p["ds"], "dl": p["dl"], "d": p["d"], "du": p["du"],
                               "dw": p["dw"], "x": x})
             if b.key[0] == "seq":
+                # like the reference's application, one buffer for every call:
+                # the reference-sized buffer of the pool's largest need
                 r, g = b.requests[0], grids[0]
-                buf = ps.alloc_buffer(ps.dims_of(g["x"]), r.solvedim, torch.float64)
+                if self._seq_buf is None:
+                    need = max(ps.buffer_size(list(d), sd, 8) for d in self.pool.shapes
+                               for sd in range(3))
+                    self._seq_buf = ps.aligned_bytes(need, x.device)
                 ps.gpsv_batch(g["ds"], g["dl"], g["d"], g["du"], g["dw"], g["x"], r.solvedim,
-                              buffer=buf, stream=s, handle=self.handle)
-                plan = buf
+                              buffer=self._seq_buf, stream=s, handle=self.handle)
+                plan = None
             else:
                 steps = self.refine_steps if b.key[1] == "mixed" else None
                 plan = ps.Plan(grids, b.key[0], refine_steps=steps, handle=self.handle)
@@ -364,9 +385,11 @@ class CudaExecutor:
             self.status[r.rid] = bits
         if hasattr(plan, "close"):
             plan.close()
-        if self.keep_results:
-            for r, g in zip(b.requests, grids):
+        for r, g in zip(b.requests, grids):
+            if self.keep_results:
                 self.results[r.rid] = g["x"]
+            else:
+                self.pool.give_back(r.problem, g["x"])
         b.handle = None
 
 
@@ -543,7 +566,7 @@ def serve_native(pool: ProblemPool, trace, policy: str, arena_bytes: float, max_
             room -= 1
             r = pending[i]
             p = pool.items[r.problem]
-            x = p["b"].clone()
+            x = pool.iterate(r.problem)
             g = {k: p[k] for k in ("ds", "dl", "d", "du", "dw")}
             g["x"] = x
             rid = srv.submit(g, r.solvedim, r.tol)
@@ -561,7 +584,7 @@ def serve_native(pool: ProblemPool, trace, policy: str, arena_bytes: float, max_
             bits[r.rid] = b
             done += 1
             if not keep_results:
-                xs.pop(rid)
+                pool.give_back(r.problem, xs.pop(rid))
         if i < len(pending) and srv.stats()["in_flight"] == 0 and not srv.stats()["queued"]:
             dt = pending[i].arrival - (time.perf_counter() - t0)
             if dt > 2e-4:
