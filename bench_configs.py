@@ -395,7 +395,8 @@ def config4(rate=2000.0, seconds=2.0, n_problems=64, budget=150e9, seed=44):
         serving.serve_native(pool, warm, policy, arena)
         torch.cuda.empty_cache()
     for label, r in (("nominal", rate), ("saturated", math.inf)):
-        trace = serving.make_trace(n_req if label == "nominal" else n_req // 2, r, n_problems,
+        # saturated: 8000 requests queued at t = 0 (about half a second of device work)
+        trace = serving.make_trace(n_req if label == "nominal" else 2 * n_req, r, n_problems,
                                    seed=seed + 1)
         res = {}
         for policy in ("mixed", "fp64", "sequential"):
