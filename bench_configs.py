@@ -399,15 +399,20 @@ def config4(rate=2000.0, seconds=2.0, n_problems=64, budget=150e9, seed=44):
         trace = serving.make_trace(n_req if label == "nominal" else 2 * n_req, r, n_problems,
                                    seed=seed + 1)
         res = {}
+
+        def fresh(run):
+            # each implementation and policy first serves the trace untimed, from
+            # empty iterate free lists, so the timed run meets its own steady state
+            pool.drop_iterates()
+            torch.cuda.empty_cache()
+            run()
+
         for policy in ("mixed", "fp64", "sequential"):
-            if label == "saturated":   # untimed: the iterate free lists reach this load
-                serving.serve(pool, trace, policy, budget)
-                serving.serve_native(pool, trace, policy, arena)
-                torch.cuda.empty_cache()
+            fresh(lambda: serving.serve(pool, trace, policy, budget))
             rep, ex, _ = serving.serve(pool, trace, policy, budget, calibrate=True)
             res[policy] = rep
             del ex
-            torch.cuda.empty_cache()
+            fresh(lambda: serving.serve_native(pool, trace, policy, arena))
             rep, _, bits, _ = serving.serve_native(pool, trace, policy, arena, calibrate=True)
             rep["status_bits_nonzero"] = sum(1 for v in bits.values() if v)
             res[f"native_{policy}"] = rep

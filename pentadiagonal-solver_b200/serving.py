@@ -250,6 +250,10 @@ class ProblemPool:
         """Return an iterate whose request's work has completed on the device."""
         self._free[i].append(x)
 
+    def drop_iterates(self) -> None:
+        """Forget the kept iterates (their memory goes back to the allocator)."""
+        self._free = [[] for _ in self.shapes]
+
     def points(self, i) -> int:
         return int(math.prod(self.shapes[i]))
 
@@ -278,6 +282,9 @@ class CudaExecutor:
         self.t0 = time.perf_counter()
         self.handle = ps.Handle()
         self._seq_buf = None   # the sequential baseline's one buffer, sized on first use
+        # FP64 plans' scratch, one growing buffer per stream: a batch's plan runs
+        # after everything queued before it on its stream, so it may reuse it
+        self._scratch = [None] * len(self.streams)
         # per solve direction: does the refined form beat plain FP64 here?
         self.calibration = self.measure_costs() if calibrate else None
 
@@ -339,7 +346,8 @@ class CudaExecutor:
 
     def launch(self, b: Batch):
         torch, ps = self.torch, self.ps
-        s = self.streams[self.next_stream]
+        si = self.next_stream
+        s = self.streams[si]
         self.next_stream = (self.next_stream + 1) % len(self.streams)
         grids = []
         with torch.cuda.stream(s):
@@ -361,7 +369,16 @@ class CudaExecutor:
                 plan = None
             else:
                 steps = self.refine_steps if b.key[1] == "mixed" else None
-                plan = ps.Plan(grids, b.key[0], refine_steps=steps, handle=self.handle)
+                scratch = None
+                if steps is None:
+                    need = ps.plan_sizes(grids, b.key[0], self.handle)[1]
+                    if self._scratch[si] is None or self._scratch[si].numel() < need:
+                        self._scratch[si] = None
+                        self._scratch[si] = ps.aligned_bytes(max(need + need // 4, 256),
+                                                             x.device)
+                    scratch = self._scratch[si]
+                plan = ps.Plan(grids, b.key[0], refine_steps=steps, handle=self.handle,
+                               scratch=scratch)
                 plan.execute(s)
             ev = torch.cuda.Event()
             ev.record(s)
