@@ -426,7 +426,9 @@ bool pick_tmem(Context &ctx, const SolveArgs<F> &a, bool contig, size_t usable_b
   for (size_t i = 0; i < all.size(); ++i) {
     const TmemConfig &c = all[i];
     if (c.contig != contig || c.fmode != fmode || c.loads != loads) continue;
-    if ((want[0] >= 0 && c.stages != want[0]) || (want[1] >= 0 && c.xstages != want[1]))
+    // factor mode 3 reads nothing back: only the ring depth of a choice applies
+    if ((want[0] >= 0 && c.stages != want[0]) ||
+        (want[1] >= 0 && fmode != 3 && c.xstages != want[1]))
       continue;
     if (c.smem > (size_t)ctx.smem_optin) continue;
     int occ;
@@ -618,7 +620,11 @@ pentadStatus_t solve(Context &ctx, const F *ds, const F *dl, const F *d,
             const char *ld = mc.loads == 1 ? tmem_loader<F>(a, contig) : "";
             std::snprintf(vb, sizeof vb, "thomas-pcr:tmem P2 S16 R%d x%d/%d%s%s%s", mc.R,
                           mc.stages, mc.xstages,
-                          mc.fmode == 2 ? " fbuf" : mc.fmode == 1 ? " w2s" : "", ld,
+                          mc.fmode == 2   ? " fbuf"
+                          : mc.fmode == 1 ? " w2s"
+                          : mc.fmode == 3 ? " x2t"
+                                          : "",
+                          ld,
                           contig ? " contig" : "");
             record(ctx, dir, "thomas-pcr", vb);
             return PENTAD_STATUS_SUCCESS;
@@ -801,11 +807,11 @@ pentadStatus_t plan_layout(Context &ctx, int count, const pentadsolver_grid_t *g
   for (int i = 0; i < count; ++i)
     if (ok[i]) {
       order.push_back(i);
-      w2s = w2s || need_w2s[i] != 0;
+      w2s = w2s || need_w2s[i] == 1 || need_w2s[i] == 2;  // factors through the buffer
     }
   // one job group per factor mode (du2 and dw2 in TMEM; du2 alone; all in
-  // the buffer) and stage layout (TMA tiles or bulk copies), each heaviest
-  // lines first
+  // the buffer; all in TMEM) and stage layout (TMA tiles or bulk copies),
+  // each heaviest lines first
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
     if (need_w2s[a] != need_w2s[b]) return need_w2s[a] < need_w2s[b];
     if (loads[a] != loads[b]) return loads[a] < loads[b];
@@ -939,12 +945,16 @@ pentadStatus_t plan_build(Context &ctx, int count, const pentadsolver_grid_t *gr
   p->ctas = (ctas > 0 && ctas < ctx.sm_count) ? ctas : ctx.sm_count;
   p->singles = singles;
   char d[160];
-  int n_bulk = 0;
-  for (int i : order) n_bulk += gloads[i] ? 1 : 0;
+  int n_bulk = 0, n_x2t = 0;
+  for (int i : order) {
+    n_bulk += gloads[i] ? 1 : 0;
+    n_x2t += gw2s[i] == 3 ? 1 : 0;
+  }
   std::snprintf(d, sizeof d,
-                "tmem-batch %s grids=%d tiles=%d launches=%d%s ctas=%d alone=%d pitched=%d",
+                "tmem-batch %s grids=%d tiles=%d launches=%d%s ctas=%d alone=%d pitched=%d "
+                "x2t=%d",
                 sizeof(F) == 8 ? "f64" : "f32", p->n_jobs, total_tiles, (int)groups.size(),
-                w2s ? " w2s" : "", p->ctas, (int)singles.size(), n_bulk);
+                w2s ? " w2s" : "", p->ctas, (int)singles.size(), n_bulk, n_x2t);
   p->desc = d;
   out = p;
   return PENTAD_STATUS_SUCCESS;

@@ -27,7 +27,11 @@
 //    a stage into registers and releases the slot at once.
 //  * Factors in Tensor Memory (lanes 32c..32c+31, the quarter these warps can
 //    reach), one tcgen05.st per stage on the way down and one tcgen05.ld per
-//    stage on the way back, in one of three factor modes FM:
+//    stage on the way back, in one of four factor modes FM:
+//      - 3, du2, dw2 and x2 all in TMEM (short lines): 6 columns per FP64
+//        row, 3 per FP32 row, 480 of the 512 columns, m <= 80 / 160 rows,
+//        n <= 160 / 320; nothing goes through the buffer, so the back
+//        substitution waits for no read-back and a call needs no buffer;
 //      - 0, du2 and dw2 in TMEM: 4 columns per FP64 row, 2 per FP32 row;
 //        512 columns hold m <= 128 (FP64) / 256 (FP32) rows, n <= 256 / 512;
 //      - 1, du2 only: half the columns, n <= 512 / 1024, with dw2 travelling
@@ -111,9 +115,15 @@ constexpr uint32_t kTmemCols = 512; // the whole of Tensor Memory
 template <typename F, bool CONTIG> constexpr int tmem_rows_per_stage() {
   return CONTIG ? 64 / (int)sizeof(F) : 1024 / (TS * (int)sizeof(F));
 }
-// TMEM columns per stage: R rows of du2, dw2 (or du2 alone), sizeof(F)/4 each.
+// Factor modes: 0 du2 and dw2 in TMEM, x2 through the buffer; 1 du2 in TMEM,
+// (dw2, x2) through the buffer; 2 all three through the buffer; 3 all three in
+// TMEM (short lines: no buffer round trip at all).
+template <typename F, int FM> __host__ __device__ constexpr int tmem_values_per_row() {
+  return FM == 0 ? 2 : FM == 3 ? 3 : 1;
+}
+// TMEM columns per stage: R rows of the values kept there, sizeof(F)/4 each.
 template <typename F, int FM> constexpr int tmem_cols_per_stage() {
-  return 64 / (int)sizeof(F) * (FM == 0 ? 2 : 1) * (int)sizeof(F) / 4;
+  return 64 / (int)sizeof(F) * tmem_values_per_row<F, FM>() * (int)sizeof(F) / 4;
 }
 
 // LD: how the forward stages are filled.  0: TMA tensor tiles of R x 16 (or,
@@ -124,7 +134,7 @@ template <typename F, int FM> constexpr int tmem_cols_per_stage() {
 template <typename F, bool CONTIG, int FM, int ST, int XST, int LD> struct TmemGeom {
   static constexpr int R = tmem_rows_per_stage<F, CONTIG>();
   static constexpr int EPC = 16 / (int)sizeof(F);     // elements per 16-byte chunk
-  static constexpr int PW = FM == 2 ? 3 : (FM == 1 ? 2 : 1);  // scratch values per row
+  static constexpr int PW = FM == 2 ? 3 : FM == 1 ? 2 : FM == 3 ? 0 : 1;  // scratch values per row
   static constexpr int BOX = R * TS;                  // elements per TMA tile
   // bulk layout pitches: a strided row of 16 lines + one chunk; a line's R rows
   // + one chunk (along x)
@@ -169,7 +179,9 @@ template <typename F, bool CONTIG, int FM, int ST, int XST, int LD> struct TmemG
                 "TMA destinations must stay 128-byte aligned");
   static_assert((PS * sizeof(F)) % 16 == 0 && (PL * sizeof(F)) % 16 == 0,
                 "bulk-copy destinations must stay 16-byte aligned");
-  static_assert(R * (FM == 0 ? 2 : 1) * (int)sizeof(F) / 4 == kCols, "TMEM columns per stage");
+  static_assert(R * tmem_values_per_row<F, FM>() * (int)sizeof(F) / 4 == kCols,
+                "TMEM columns per stage");
+  static_assert(kCols == 16 || kCols == 32 || kCols == 48, "a TMEM load or store per stage");
 };
 
 template <typename F> __device__ __forceinline__ void put_bits(uint32_t *tv, int c, F v);
@@ -722,12 +734,14 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         for (int r = 0; r < R; ++r)
           fwd_row_lean(a[r][0], a[r][1], a[r][2], a[r][3], a[r][4], a[r][5], c, u[r], w[r],
                        y[r]);
-        if constexpr (FM < 2) {  // du2 (and dw2) into TMEM
+        if constexpr (FM != 2) {  // du2 (and dw2, and x2) into TMEM
+        constexpr int VPR = tmem_values_per_row<F, FM>();
         uint32_t tv[G::kCols];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          put_bits<F>(tv, r * CW * (FM == 0 ? 2 : 1), u[r]);
-          if (FM == 0) put_bits<F>(tv, r * CW * 2 + CW, w[r]);
+          put_bits<F>(tv, r * CW * VPR, u[r]);
+          if (VPR >= 2) put_bits<F>(tv, r * CW * VPR + CW, w[r]);
+          if (VPR == 3) put_bits<F>(tv, r * CW * VPR + 2 * CW, y[r]);
         }
         // wait (lane 0, bounded) until the previous tile has read this block
         const int need = (ti - 1) * 65536 + max(0, g + 1 - free_blocks);
@@ -758,7 +772,9 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         }
         tmem_fence_after_sync();
         const int blk = flip ? NB - 1 - g : g;
-        if constexpr (G::kCols == 32)
+        if constexpr (G::kCols == 48)
+          tmem_store48(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[48]>(tv));
+        else if constexpr (G::kCols == 32)
           tmem_store32(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[32]>(tv));
         else
           tmem_store16(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[16]>(tv));
@@ -766,7 +782,9 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         F *const x2g = x2w + g * R * TS * PW;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          if constexpr (FM == 2) {
+          if constexpr (FM == 3) {
+            // nothing leaves the SM: x2 went to TMEM with the factors
+          } else if constexpr (FM == 2) {
             st_hint(x2g + (3 * r) * TS, u[r], pol_x2);
             st_hint(x2g + (3 * r + 1) * TS, w[r], pol_x2);
             st_hint(x2g + (3 * r + 2) * TS, y[r], pol_x2);
@@ -893,7 +911,8 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         ++r_issued;
         if (++ri_slot == XST) ri_slot = 0;
       };
-      for (int s = 0; s < XST; ++s) rissue(s);
+      if constexpr (FM != 3)  // factor mode 3 keeps x2 in TMEM: nothing to read back
+        for (int s = 0; s < XST; ++s) rissue(s);
 
       // ---------------------------- interface -------------------------------
       const F *const h = hand + (ti & 1) * 6 * 32 + lane;
@@ -926,8 +945,10 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         const int g = n_stages - 1 - s;  // the forward stage being undone
         const int blk = flip ? NB - 1 - g : g;
         uint32_t tv[G::kCols];
-        if constexpr (FM < 2) {
-          if constexpr (G::kCols == 32)
+        if constexpr (FM != 2) {
+          if constexpr (G::kCols == 48)
+            tmem_load48(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[48]>(tv));
+          else if constexpr (G::kCols == 32)
             tmem_load32(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[32]>(tv));
           else
             tmem_load16(taddr + (uint32_t)(blk * G::kCols), reinterpret_cast<uint32_t(&)[16]>(tv));
@@ -936,9 +957,11 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
           __syncwarp();
           if (lane == 0) st_release_shared(&prog[cons], ti * 65536 + s + 1);
         }
-        if (!__all_sync(0xffffffffu, mbar_wait(&rfull[r_slot], r_phase))) {
-          fail = 1;
-          break;
+        if constexpr (FM != 3) {
+          if (!__all_sync(0xffffffffu, mbar_wait(&rfull[r_slot], r_phase))) {
+            fail = 1;
+            break;
+          }
         }
         const F *xsrc = xr + r_slot * XE +
                         (FM == 2 ? part * R * TS * PW + sys : (part * R * TS + sys) * PW);
@@ -946,7 +969,11 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int j = R - 1 - r;  // row inside the stage block
-          if constexpr (FM == 2) {
+          if constexpr (FM == 3) {
+            du[r] = get_bits<F>(tv, j * CW * 3);
+            dw[r] = get_bits<F>(tv, j * CW * 3 + CW);
+            xs[r] = get_bits<F>(tv, j * CW * 3 + 2 * CW);
+          } else if constexpr (FM == 2) {
             du[r] = xsrc[(3 * j) * TS];
             dw[r] = xsrc[(3 * j + 1) * TS];
             xs[r] = xsrc[(3 * j + 2) * TS];
@@ -964,11 +991,13 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
         if (CONTIG && (s & 1) == 0 && lane == 0) bulk_wait_read<1>();  // buffer o_buf is free
         fence_async_shared();
         __syncwarp();
-        ++r_consumed;
-        rissue(s + XST);  // refills the slot just read (ri_slot == r_slot here)
-        if (++r_slot == XST) {
-          r_slot = 0;
-          r_phase ^= 1u;
+        if constexpr (FM != 3) {
+          ++r_consumed;
+          rissue(s + XST);  // refills the slot just read (ri_slot == r_slot here)
+          if (++r_slot == XST) {
+            r_slot = 0;
+            r_phase ^= 1u;
+          }
         }
         // the stage's block of each half is dead: drop its 128-byte lines
         constexpr int kLines = (int)(kBlock / 128);
@@ -1024,6 +1053,10 @@ tmem_thomas_kernel(const __grid_constant__ TmemJob<F> job1, const TmemJob<F> *__
                 tma_store_2d_hint(&J->maps[5], ob + 2 * BOX, mt + s * R, c0, pol_out);
               bulk_commit();
             }
+            // the next tile writes the other buffer: the wait before each
+            // even step leaves one store group in flight, and that group may
+            // still be reading this one
+            o_buf ^= 1;
           } else {
             const int odd = (s & 1) ? R : 0;
 #pragma unroll
@@ -1138,9 +1171,15 @@ bool shape_ok(const Lines &L, bool contig, int &fmode) {
   const long long mt = split_row<F>(L, contig);
   if (L.n - mt < 2) return false;  // two real rows per half
   const long long stages = mt / R;
+  const long long cap_all = kTmemCols / tmem_cols_per_stage<F, 3>();
   const long long cap_both = kTmemCols / tmem_cols_per_stage<F, 0>();
   const long long cap_du = kTmemCols / tmem_cols_per_stage<F, 1>();
-  fmode = stages > cap_du ? 2 : stages > cap_both ? 1 : 0;
+  // PENTA_TMEM_FM3=0: short lines too send x2 through the buffer (measurement)
+  static const bool fm3_off = [] {
+    const char *e = std::getenv("PENTA_TMEM_FM3");
+    return e != nullptr && e[0] == '0';
+  }();
+  fmode = stages > cap_du ? 2 : stages > cap_both ? 1 : (stages <= cap_all && !fm3_off) ? 3 : 0;
   // every global offset is formed in 64 bits; line, run and tile indices (and
   // the TMA coordinates made of them) must stay below 2^31
   if (L.n_sys >= (1LL << 31) - TS || tile_count(L, contig) >= (1LL << 31)) return false;
@@ -1168,7 +1207,7 @@ template <typename F> bool tma_ok(const SolveArgs<F> &a, bool contig) {
 
 template <typename F> size_t job_scratch_bytes(const Lines &L, bool contig, int fmode) {
   return (size_t)tile_count(L, contig) * 2 * (size_t)split_row<F>(L, contig) * TS *
-         (fmode == 2 ? 3 : fmode == 1 ? 2 : 1) * sizeof(F);
+         (fmode == 2 ? 3 : fmode == 1 ? 2 : fmode == 3 ? 0 : 1) * sizeof(F);
 }
 
 // The pitched layout filled by 16-byte cp.async copies: the default for
@@ -1353,7 +1392,19 @@ template <typename F, bool CONTIG, int FM, int ST, int XST, int LD> int tmem_occ
   X(float, true, 1, 2, 2, 1)    \
   X(float, false, 1, 2, 4, 1)   \
   X(float, true, 2, 2, 1, 1)    \
-  X(float, false, 2, 2, 2, 1)
+  X(float, false, 2, 2, 2, 1)   \
+  X(double, true, 3, 2, 1, 0)   \
+  X(double, true, 3, 3, 1, 0)   \
+  X(double, false, 3, 3, 1, 0)  \
+  X(double, false, 3, 2, 1, 0)  \
+  X(float, true, 3, 3, 1, 0)    \
+  X(float, true, 3, 2, 1, 0)    \
+  X(float, false, 3, 3, 1, 0)   \
+  X(float, false, 3, 4, 1, 0)   \
+  X(double, true, 3, 2, 1, 1)   \
+  X(double, false, 3, 3, 1, 1)  \
+  X(float, true, 3, 2, 1, 1)    \
+  X(float, false, 3, 2, 1, 1)
 
 template <typename F> const std::vector<TmemConfig> &tmem_configs() {
   static const std::vector<TmemConfig> v = [] {
@@ -1419,8 +1470,9 @@ template <typename F> const char *tmem_loader(const SolveArgs<F> &a, bool contig
 template <typename F>
 bool tmem_supported(const SolveArgs<F> &a, bool contig, size_t usable_buf, int &fmode) {
   if (!tmem_shape<F>(a.L, contig, fmode)) return false;
-  if (a.scratch == nullptr || reinterpret_cast<uintptr_t>(a.scratch) % 16 != 0 ||
-      tmem_scratch_bytes<F>(a.L, contig, fmode) > usable_buf)
+  // factor mode 3 keeps everything on chip: it needs no buffer at all
+  if (fmode != 3 && (a.scratch == nullptr || reinterpret_cast<uintptr_t>(a.scratch) % 16 != 0 ||
+                     tmem_scratch_bytes<F>(a.L, contig, fmode) > usable_buf))
     return false;
   const void *ptrs[6] = {a.ds, a.dl, a.d, a.du, a.dw, a.x};
   for (const void *p : ptrs)  // element alignment (TMA needs 16 bytes; see tma_ok)

@@ -262,8 +262,9 @@ def _tmem_ok(dims, solvedim, eb):
     (y, z) are 16-byte aligned, element copies otherwise): two real rows in
     each half of the split m = R ceil(n / 2R), and its scratch for whole tiles
     of 16 lines within the reference-sized buffer.  The factor mode follows
-    the m / R stages: du2 and dw2 in 512 TMEM columns (16 stages), du2 alone
-    with dw2 in the buffer (32 stages), or all factors in the buffer."""
+    the m / R stages: du2, dw2 and x2 all in 512 TMEM columns (10 stages, no
+    scratch), du2 and dw2 (16 stages), du2 alone with dw2 in the buffer (32
+    stages), or all factors in the buffer."""
     n = dims[solvedim]
     inner = int(np.prod(dims[:solvedim]))
     n_sys = int(np.prod(dims)) // n
@@ -273,11 +274,20 @@ def _tmem_ok(dims, solvedim, eb):
     mt = r * (-(-n // (2 * r)))
     stages = mt // r
     cols = r * eb // 4               # TMEM columns of one factor per stage
-    per_row = 1 if stages <= 512 // (2 * cols) else 2 if stages <= 512 // cols else 3
+    per_row = (0 if stages <= 512 // (3 * cols) else 1 if stages <= 512 // (2 * cols)
+               else 2 if stages <= 512 // cols else 3)
     tiles = -(-n_sys // 16) if contig else (n_sys // inner) * -(-inner // 16)
     need = tiles * 2 * mt * 16 * eb * per_row
     buf = ps.buffer_size(list(dims), solvedim, eb)
     return aligned and n - mt >= 2 and need <= buf
+
+
+def _x2_on_chip(dims, solvedim, eb):
+    """Lines short enough that the Tensor-Memory kernel keeps x2 in TMEM too
+    (10 stages of R rows per half): it needs no buffer at all."""
+    n = dims[solvedim]
+    r = 64 // eb if solvedim == 0 else 1024 // (16 * eb)
+    return -(-n // (2 * r)) <= 10
 
 
 def _old_tma_ok(dims, solvedim, eb, buffer=True):
@@ -350,11 +360,14 @@ def test_kernel_chain_every_direction(cuda, dims, dtype, monkeypatch):
         v = check((), offset=16)
         assert ("tmem" in v) == tm, (solvedim, v)
         # 8-byte aligned: no buffer-using TMA kernel (the strided one keeps its
-        # factors on chip and still runs)
+        # factors on chip and still runs); lines whose factors and x2 all stay
+        # in TMEM need no buffer, so the Tensor-Memory kernel runs regardless
+        on_chip = tm and _x2_on_chip(dims, solvedim, eb)
         v = check((), offset=8)
-        assert "tmem" not in v and ("tma" in v) == (old and solvedim != 0), (solvedim, v)
+        assert ("tmem" in v) == on_chip, (solvedim, v)
+        assert on_chip or ("tma" in v) == (old and solvedim != 0), (solvedim, v)
         v = check((), buffer=False)
-        assert "tmem" not in v, (solvedim, v)
+        assert ("tmem" in v) == on_chip, (solvedim, v)
 
 
 LONG_DIMS = [((1040, 16, 5), 0), ((16, 1104, 5), 1), ((16, 5, 1040), 2), ((1033, 16, 5), 0),

@@ -104,7 +104,9 @@ def test_native_server_respects_a_small_arena(cuda):
 def test_native_server_rejects_a_request_larger_than_its_arena(cuda):
     import torch
 
-    pool = serving.ProblemPool([(128, 128, 64)], seed=51)   # plan scratch of several MB
+    # lines of 256 along x: x2 goes through the plan's scratch (16 MB here);
+    # lines of at most 160 would keep everything in Tensor Memory and fit
+    pool = serving.ProblemPool([(256, 128, 64)], seed=51)
     srv = serving.NativeServer(1 << 20, "fp64")   # 1 MiB: the grid's plan cannot fit
     p = pool.items[0]
     rid = srv.submit({**{k: p[k] for k in ("ds", "dl", "d", "du", "dw")}, "x": p["b"].clone()},
