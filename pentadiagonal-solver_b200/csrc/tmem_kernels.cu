@@ -29,9 +29,10 @@
 //    reach), one tcgen05.st per stage on the way down and one tcgen05.ld per
 //    stage on the way back, in one of four factor modes FM:
 //      - 3, du2, dw2 and x2 all in TMEM (short lines): 6 columns per FP64
-//        row, 3 per FP32 row, 480 of the 512 columns, m <= 80 / 160 rows,
-//        n <= 160 / 320; nothing goes through the buffer, so the back
-//        substitution waits for no read-back and a call needs no buffer;
+//        row, 3 per FP32 row, 10 blocks of a stage in 480 of the 512
+//        columns, used up to 8 stages: m <= 64 / 128 rows, n <= 128 / 256;
+//        nothing goes through the buffer, so the back substitution waits for
+//        no read-back and a call needs no buffer;
 //      - 0, du2 and dw2 in TMEM: 4 columns per FP64 row, 2 per FP32 row;
 //        512 columns hold m <= 128 (FP64) / 256 (FP32) rows, n <= 256 / 512;
 //      - 1, du2 only: half the columns, n <= 512 / 1024, with dw2 travelling
@@ -1171,7 +1172,10 @@ bool shape_ok(const Lines &L, bool contig, int &fmode) {
   const long long mt = split_row<F>(L, contig);
   if (L.n - mt < 2) return false;  // two real rows per half
   const long long stages = mt / R;
-  const long long cap_all = kTmemCols / tmem_cols_per_stage<F, 3>();
+  // all three values fit 10 stages, but with all 10 in use the next tile's
+  // forward sweep waits for every block in turn (160^3 FP64: 1-6% slower than
+  // factor mode 0); at 8 stages it gains (128^3: 11-14%)
+  const long long cap_all = kTmemCols / tmem_cols_per_stage<F, 3>() - 2;
   const long long cap_both = kTmemCols / tmem_cols_per_stage<F, 0>();
   const long long cap_du = kTmemCols / tmem_cols_per_stage<F, 1>();
   // PENTA_TMEM_FM3=0: short lines too send x2 through the buffer (measurement)

@@ -262,7 +262,7 @@ def _tmem_ok(dims, solvedim, eb):
     (y, z) are 16-byte aligned, element copies otherwise): two real rows in
     each half of the split m = R ceil(n / 2R), and its scratch for whole tiles
     of 16 lines within the reference-sized buffer.  The factor mode follows
-    the m / R stages: du2, dw2 and x2 all in 512 TMEM columns (10 stages, no
+    the m / R stages: du2, dw2 and x2 all in TMEM (up to 8 stages, no
     scratch), du2 and dw2 (16 stages), du2 alone with dw2 in the buffer (32
     stages), or all factors in the buffer."""
     n = dims[solvedim]
@@ -274,7 +274,7 @@ def _tmem_ok(dims, solvedim, eb):
     mt = r * (-(-n // (2 * r)))
     stages = mt // r
     cols = r * eb // 4               # TMEM columns of one factor per stage
-    per_row = (0 if stages <= 512 // (3 * cols) else 1 if stages <= 512 // (2 * cols)
+    per_row = (0 if stages <= 512 // (3 * cols) - 2 else 1 if stages <= 512 // (2 * cols)
                else 2 if stages <= 512 // cols else 3)
     tiles = -(-n_sys // 16) if contig else (n_sys // inner) * -(-inner // 16)
     need = tiles * 2 * mt * 16 * eb * per_row
@@ -284,10 +284,10 @@ def _tmem_ok(dims, solvedim, eb):
 
 def _x2_on_chip(dims, solvedim, eb):
     """Lines short enough that the Tensor-Memory kernel keeps x2 in TMEM too
-    (10 stages of R rows per half): it needs no buffer at all."""
+    (up to 8 stages of R rows per half): it needs no buffer at all."""
     n = dims[solvedim]
     r = 64 // eb if solvedim == 0 else 1024 // (16 * eb)
-    return -(-n // (2 * r)) <= 10
+    return -(-n // (2 * r)) <= 8
 
 
 def _old_tma_ok(dims, solvedim, eb, buffer=True):
