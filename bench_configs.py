@@ -168,7 +168,8 @@ def config0():
         for axis in range(3):
             x0 = dv["x"].clone()
             ms = timed(lambda: (dv["x"].copy_(x0), ps.gpsv_batch(*(dv[k] for k in NAMES), axis,
-                                                                  handle=h)))
+                                                                  handle=h)),
+                       reps=100, warmup=10)
             dv["x"].copy_(x0)
             ps.gpsv_batch(*(dv[k] for k in NAMES), axis, handle=h)
             oracle.solve(co["ds"], co["dl"], co["d"], co["du"], co["dw"], ref, axis)
