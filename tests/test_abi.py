@@ -173,3 +173,22 @@ def test_adi_graph_refuses_bad_arguments_before_touching_a_device():
         st = f(None, eb, *a, dims, nd, it, buf, nbytes, None if o is None else ctypes.byref(o))
         assert st == ps.INVALID_VALUE, (eb, nd, it, buf, nbytes)
         assert not out.value
+
+
+def test_plan_entry_points_refuse_bad_arguments_on_host():
+    # plan execution, description, status and destruction take a NULL plan as
+    # invalid; pentadsolver_plan_execute_ex also refuses unknown flag bits
+    import ctypes
+
+    import pentadsolver as ps
+
+    exe = ps._typed("pentadsolver_plan_execute", [ctypes.c_void_p, ctypes.c_void_p])
+    exe_ex = ps._typed("pentadsolver_plan_execute_ex",
+                       [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int])
+    destroy = ps._typed("pentadsolver_plan_destroy", [ctypes.c_void_p])
+    describe = ps._typed("pentadsolver_plan_describe", [ctypes.c_void_p], ctypes.c_char_p)
+    assert exe(None, None) == ps.INVALID_VALUE
+    for flags in (0, 1, 2, -1):
+        assert exe_ex(None, None, flags) == ps.INVALID_VALUE
+    assert destroy(None) == ps.INVALID_VALUE
+    assert describe(None) == b"none"
