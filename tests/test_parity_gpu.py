@@ -461,3 +461,23 @@ def test_bulk_loads_on_aligned_grids_equal_tma_tiles(cuda, dtype, monkeypatch):
             x_bulk, v_bulk = _loads_run(co, solvedim, "bulk", monkeypatch)
             assert "tmem" in v_tma and "bulk" not in v_tma and "bulk" in v_bulk, (v_tma, v_bulk)
             assert np.array_equal(x_tma.view(np.uint8), x_bulk.view(np.uint8)), (dims, solvedim)
+
+
+# x lines whose halves take an odd number of stages: the last step of every tile
+# leaves through the shared output buffer without a partner step, and the next
+# tile must not write that buffer while its store may still be reading it
+ODD_STAGE_X = [((24, 300, 40), np.float32),   # 1 stage (16 rows a stage), all in TMEM
+               ((40, 300, 40), np.float64),   # 3 stages (8 rows), all in TMEM
+               ((200, 100, 20), np.float64),  # 13 stages, x2 through the buffer
+               ((400, 60, 20), np.float32)]   # 13 stages
+
+
+@pytest.mark.parametrize("dims,dtype", ODD_STAGE_X)
+def test_x_tiles_with_an_odd_number_of_stages(cuda, dims, dtype):
+    co = fixtures.random_dominant(dims, 91, dtype)
+    ref = {k: co[k].astype(np.float64) for k in NAMES}
+    oracle.solve(ref["ds"], ref["dl"], ref["d"], ref["du"], ref["dw"], ref["x"], 0)
+    for _ in range(5):
+        dv = to_dev(co)
+        solve_dev(dv, 0)
+        assert fwd_err(dv["x"].cpu().numpy(), ref["x"]) <= FWD_TOL[dtype], dims
