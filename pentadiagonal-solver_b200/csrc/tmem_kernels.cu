@@ -30,7 +30,8 @@
 //    stage on the way back, in one of four factor modes FM:
 //      - 3, du2, dw2 and x2 all in TMEM (short lines): 6 columns per FP64
 //        row, 3 per FP32 row, 10 blocks of a stage in 480 of the 512
-//        columns, used up to 8 stages: m <= 64 / 128 rows, n <= 128 / 256;
+//        columns, used up to 8 stages (4 for FP32 along y/z): n <= 128 FP64,
+//        256 FP32 along x, 128 FP32 along y/z;
 //        nothing goes through the buffer, so the back substitution waits for
 //        no read-back and a call needs no buffer;
 //      - 0, du2 and dw2 in TMEM: 4 columns per FP64 row, 2 per FP32 row;
@@ -1174,8 +1175,11 @@ bool shape_ok(const Lines &L, bool contig, int &fmode) {
   const long long stages = mt / R;
   // all three values fit 10 stages, but with all 10 in use the next tile's
   // forward sweep waits for every block in turn (160^3 FP64: 1-6% slower than
-  // factor mode 0); at 8 stages it gains (128^3: 11-14%)
-  const long long cap_all = kTmemCols / tmem_cols_per_stage<F, 3>() - 2;
+  // factor mode 0); at 8 stages it gains (128^3 FP64: 11-14%; FP32 along x
+  // 1-3% up to 256 rows).  FP32 along y and z, where x2 costs only 4 B/pt,
+  // measured 5-12% slower at 6-7 stages (192^3, 224^3): there up to 4 stages.
+  const long long cap_all =
+      (sizeof(F) == 4 && !contig) ? 4 : kTmemCols / tmem_cols_per_stage<F, 3>() - 2;
   const long long cap_both = kTmemCols / tmem_cols_per_stage<F, 0>();
   const long long cap_du = kTmemCols / tmem_cols_per_stage<F, 1>();
   // PENTA_TMEM_FM3=0: short lines too send x2 through the buffer (measurement)

@@ -274,7 +274,8 @@ def _tmem_ok(dims, solvedim, eb):
     mt = r * (-(-n // (2 * r)))
     stages = mt // r
     cols = r * eb // 4               # TMEM columns of one factor per stage
-    per_row = (0 if stages <= 512 // (3 * cols) - 2 else 1 if stages <= 512 // (2 * cols)
+    cap_all = 4 if (eb == 4 and not contig) else 512 // (3 * cols) - 2
+    per_row = (0 if stages <= cap_all else 1 if stages <= 512 // (2 * cols)
                else 2 if stages <= 512 // cols else 3)
     tiles = -(-n_sys // 16) if contig else (n_sys // inner) * -(-inner // 16)
     need = tiles * 2 * mt * 16 * eb * per_row
@@ -284,10 +285,11 @@ def _tmem_ok(dims, solvedim, eb):
 
 def _x2_on_chip(dims, solvedim, eb):
     """Lines short enough that the Tensor-Memory kernel keeps x2 in TMEM too
-    (up to 8 stages of R rows per half): it needs no buffer at all."""
+    (up to 8 stages of R rows per half, 4 for FP32 along y/z): it needs no
+    buffer at all."""
     n = dims[solvedim]
     r = 64 // eb if solvedim == 0 else 1024 // (16 * eb)
-    return -(-n // (2 * r)) <= 8
+    return -(-n // (2 * r)) <= (4 if (eb == 4 and solvedim != 0) else 8)
 
 
 def _old_tma_ok(dims, solvedim, eb, buffer=True):
